@@ -1,0 +1,628 @@
+// The libhalf C ABI (include/half.h, include/half_b200.h).
+//
+// Handle registry, status and error-string conventions follow
+// src/half_c_api.F90: at most 32 live contexts, handle = generation*32 + slot
+// (:13-16, 208-209, 627-634), "invalid HALF context handle" for stale or
+// unknown handles (:636-640), error buffers cleared on entry and filled
+// NUL-terminated and truncated to capacity-1 (:650-665), and the mapped
+// solve's open-addressing G-vector hash with the same multipliers
+// (:521-597).  Backend/solver validation follows src/half_library.F90:51-110:
+// this build has the CUDA backend only (the reference's CPU backend needs
+// oneMKL), so CPU contexts answer HALF_ERROR_UNAVAILABLE.  Device failures
+// return HALF_ERROR_INTERNAL with a message instead of stopping the process.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "../../include/half_b200.h"
+#include "context.h"
+
+using namespace hb;
+
+namespace {
+
+constexpr int kMaxContexts = 32;
+
+struct Slot {
+  bool used = false;
+  long long generation = 0;
+  std::unique_ptr<Context> ctx;
+};
+Slot g_slots[kMaxContexts];
+std::mutex g_mutex;
+
+void clear_error(char* e, int cap) {
+  if (e && cap > 0) e[0] = '\0';
+}
+
+void export_error(const std::string& msg, char* e, int cap) {
+  if (!e || cap <= 0) return;
+  std::string m = msg;
+  while (!m.empty() && m.back() == ' ') m.pop_back();
+  size_t n = std::min(m.size(), size_t(cap - 1));
+  std::memcpy(e, m.data(), n);
+  e[n] = '\0';
+}
+
+int slot_of(half_handle h) {
+  if (h <= 0) return -1;
+  long long s = h % kMaxContexts;
+  if (s == 0) s = kMaxContexts;
+  long long g = (h - s) / kMaxContexts;
+  int idx = int(s - 1);
+  if (!g_slots[idx].used || g != g_slots[idx].generation) return -1;
+  return idx;
+}
+
+Context* lookup(half_handle h) {
+  int s = slot_of(h);
+  return s < 0 ? nullptr : g_slots[s].ctx.get();
+}
+
+int bad_handle(char* e, int cap) {
+  export_error("invalid HALF context handle", e, cap);
+  return HALF_ERROR_INVALID_HANDLE;
+}
+
+template <typename F>
+int guarded(char* e, int cap, F&& f) {
+  try {
+    return f();
+  } catch (const Error& err) {
+    export_error(err.what(), e, cap);
+    return err.status;
+  } catch (const std::bad_alloc&) {
+    export_error("host allocation failed", e, cap);
+    return HALF_ERROR_INTERNAL;
+  } catch (const std::exception& ex) {
+    export_error(std::string("internal error: ") + ex.what(), e, cap);
+    return HALF_ERROR_INTERNAL;
+  }
+}
+
+std::string cstr(const char* s) {
+  if (!s) return std::string();
+  size_t n = 0;
+  while (n < 4096 && s[n]) ++n;
+  return std::string(s, n);
+}
+
+bool finite3(const double k[3]) { return k && std::isfinite(k[0]) && std::isfinite(k[1]) && std::isfinite(k[2]); }
+
+double det3(const double* a) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+
+bool cuda_available() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) { cudaGetLastError(); return false; }
+  return n > 0;
+}
+
+int create_context(const std::string& charge, const std::string& potential, double encut, int xc, int use_uspp,
+                   int backend, int solver, half_handle* handle, char* err, int cap) {
+  if (handle) *handle = 0;
+  return guarded(err, cap, [&]() -> int {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int slot = -1;
+    for (int i = 0; i < kMaxContexts; ++i)
+      if (!g_slots[i].used) { slot = i; break; }
+    if (slot < 0) { export_error("HALF context registry is full", err, cap); return HALF_ERROR_INTERNAL; }
+    // src/half_library.F90:62-95
+    if (!(encut > 0) || !std::isfinite(encut)) fail(kInvalidArgument, "ENCUT must be positive and finite");
+    int be = backend == HALF_BACKEND_AUTO ? HALF_BACKEND_CUDA : backend;
+    if (be == HALF_BACKEND_CPU) fail(kUnavailable, "CPU API backend is not built in this B200 library; use CUDA");
+    if (!cuda_available()) fail(kUnavailable, "CUDA backend: no CUDA device is available");
+    if (!file_exists(charge)) fail(kIO, "charge input does not exist");
+    if (!file_exists(potential)) fail(kIO, "potential input does not exist");
+    auto ctx = std::make_unique<Context>();
+    read_chgcar(charge, ctx->crystal, ctx->charge);
+    ctx->pots = read_potcar(potential);
+    validate_potcar_structure(ctx->pots, ctx->crystal);
+    ctx->encut = encut;
+    ctx->use_pbe = xc == HALF_XC_PBE;
+    ctx->use_uspp = use_uspp != 0;
+    ctx->backend = be;
+    ctx->solver = solver;
+    ctx->initialize();
+    g_slots[slot].used = true;
+    g_slots[slot].generation += 1;
+    g_slots[slot].ctx = std::move(ctx);
+    if (handle) *handle = g_slots[slot].generation * kMaxContexts + (slot + 1);
+    return HALF_SUCCESS;
+  });
+}
+
+// Solve one k point with the context's solver; out holds device vectors.
+void solve_one(Context& ctx, const double k[3], int nbands, bool want_vectors, SolveOutput& out,
+               std::unique_ptr<KOperatorSet>* keep = nullptr) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (!finite3(k)) fail(kInvalidArgument, "k point must be finite");
+  bool mixed = ctx.solver == HALF_SOLVER_ACC && ctx.acc.precision == kMixed;
+  auto ks = prepare_operator(ctx, k, true, mixed);
+  double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (nbands < 1 || nbands > ks->basis.npw()) fail(kInvalidArgument, "invalid requested band count");
+  switch (ctx.solver) {
+    case HALF_SOLVER_ACC: solve_acc(ctx, *ks, nbands, want_vectors, out); break;
+    case HALF_SOLVER_EVD: solve_dense(ctx, *ks, nbands, false, want_vectors, out); ctx.last = SolveInfo(); break;
+    case HALF_SOLVER_VASP: solve_dense(ctx, *ks, nbands, true, want_vectors, out); ctx.last = SolveInfo(); break;
+    default: fail(kUnavailable, "the EVJ (Jacobi) dense solver is not built in this B200 library; use EVD, VASP or ACC");
+  }
+  ctx.last.setup_ms = setup_ms;
+  ctx.last.npw = ks->basis.npw();
+  if (keep) *keep = std::move(ks);
+}
+
+}  // namespace
+
+extern "C" {
+
+int half_get_abi_version(void) { return HALF_ABI_VERSION; }
+
+const char* half_get_version_string(void) { return "0.6.0"; }
+
+int half_get_capabilities(void) { return cuda_available() ? HALF_CAP_CUDA : 0; }
+
+int half_escn_health(const char*, int, char* error, int cap) {
+  clear_error(error, cap);
+  export_error("DeePAW-eSCN density service is not part of this build", error, cap);
+  return HALF_ERROR_UNAVAILABLE;
+}
+
+int half_escn_predict(const char*, const half_escn_request_v1*, half_escn_result_v1*, int, char* error, int cap) {
+  clear_error(error, cap);
+  export_error("DeePAW-eSCN density service is not part of this build", error, cap);
+  return HALF_ERROR_UNAVAILABLE;
+}
+
+int half_create_from_files(const char* charge, const char* potential, double encut, int xc, int use_uspp,
+                           half_handle* handle, char* error, int cap) {
+  clear_error(error, cap);
+  if (handle) *handle = 0;
+  std::string c = cstr(charge), p = cstr(potential);
+  if (c.empty() || p.empty() || (xc != 1 && xc != 2)) {
+    export_error("invalid path or XC selector", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return create_context(c, p, encut, xc, use_uspp, HALF_BACKEND_AUTO, HALF_SOLVER_EVD, handle, error, cap);
+}
+
+int half_create_from_files_backend(const char* charge, const char* potential, double encut, int xc, int use_uspp,
+                                   int backend, int solver, half_handle* handle, char* error, int cap) {
+  clear_error(error, cap);
+  if (handle) *handle = 0;
+  std::string c = cstr(charge), p = cstr(potential);
+  if (c.empty() || p.empty() || (xc != 1 && xc != 2) || backend < 0 || backend > 2 || solver < 1 || solver > 4) {
+    export_error("invalid path, XC, backend, or solver selector", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return create_context(c, p, encut, xc, use_uspp, backend, solver, handle, error, cap);
+}
+
+int half_create_from_escn(const char* url, const char* potential, const half_request_geometry_v1* geometry, double,
+                          int xc, int, int backend, int solver, int normalization, int, half_handle* handle,
+                          char* error, int cap) {
+  clear_error(error, cap);
+  if (handle) *handle = 0;
+  if (cstr(url).empty() || cstr(potential).empty() || !geometry || (xc != 1 && xc != 2) || backend < 0 ||
+      backend > 2 || solver < 1 || solver > 4 || (normalization != 0 && normalization != 1)) {
+    export_error("invalid eSCN URL, path, geometry, execution policy, or normalization", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  export_error("DeePAW-eSCN density service is not part of this build", error, cap);
+  return HALF_ERROR_UNAVAILABLE;
+}
+
+int half_destroy(half_handle handle, char* error, int cap) {
+  clear_error(error, cap);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int s = slot_of(handle);
+  if (s < 0) return bad_handle(error, cap);
+  return guarded(error, cap, [&]() -> int {
+    g_slots[s].ctx.reset();
+    g_slots[s].used = false;
+    return HALF_SUCCESS;
+  });
+}
+
+int half_set_request_geometry(half_handle handle, const half_request_geometry_v1* g, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!g) { export_error("request geometry pointer is required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  if (g->struct_size < sizeof(half_request_geometry_v1) || g->flags != 0) {
+    export_error("unsupported request geometry structure size or flags", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  if (g->nions < 1 || g->ntypes < 1 || !g->species || !g->positions_fractional) {
+    export_error("request geometry arrays and positive dimensions are required", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  // src/half_library.F90:227-247
+  if (g->grid[0] < 1 || g->grid[1] < 1 || g->grid[2] < 1) {
+    export_error("invalid request geometry dimensions", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  for (int i = 0; i < g->nions; ++i)
+    if (g->species[i] < 1 || g->species[i] > g->ntypes) {
+      export_error("invalid request geometry values", error, cap);
+      return HALF_ERROR_INVALID_ARGUMENT;
+    }
+  for (int i = 0; i < 9; ++i)
+    if (std::isnan(g->lattice[i])) { export_error("invalid request geometry values", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  for (int i = 0; i < 3 * g->nions; ++i)
+    if (std::isnan(g->positions_fractional[i])) {
+      export_error("invalid request geometry values", error, cap);
+      return HALF_ERROR_INVALID_ARGUMENT;
+    }
+  if (std::fabs(det3(g->lattice)) < 1.0e-12) { export_error("request lattice is singular", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  ctx->request_nions = g->nions;
+  ctx->request_ntypes = g->ntypes;
+  for (int i = 0; i < 3; ++i) ctx->request_grid[i] = g->grid[i];
+  for (int i = 0; i < 9; ++i) ctx->request_lattice[i] = g->lattice[i];
+  ctx->request_species.assign(g->species, g->species + g->nions);
+  ctx->request_positions.assign(g->positions_fractional, g->positions_fractional + 3 * g->nions);
+  ctx->has_request_geometry = true;
+  return HALF_SUCCESS;
+}
+
+int half_get_request_geometry(half_handle handle, int32_t* nions, int32_t* ntypes, int32_t grid[3], double lattice[9],
+                              int64_t species_capacity, int32_t* species, int64_t positions_capacity,
+                              double* positions, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!ctx->has_request_geometry) { export_error("request geometry has not been set", error, cap); return HALF_ERROR_UNAVAILABLE; }
+  if (!nions || !ntypes) { export_error("nions and ntypes output pointers are required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  *nions = ctx->request_nions;
+  *ntypes = ctx->request_ntypes;
+  if (grid) for (int i = 0; i < 3; ++i) grid[i] = ctx->request_grid[i];
+  if (lattice) for (int i = 0; i < 9; ++i) lattice[i] = ctx->request_lattice[i];
+  if (species) {
+    if (species_capacity < ctx->request_nions) { export_error("request species output capacity is too small", error, cap); return HALF_ERROR_CAPACITY; }
+    std::copy(ctx->request_species.begin(), ctx->request_species.end(), species);
+  }
+  if (positions) {
+    if (positions_capacity < 3LL * ctx->request_nions) { export_error("request positions output capacity is too small", error, cap); return HALF_ERROR_CAPACITY; }
+    std::copy(ctx->request_positions.begin(), ctx->request_positions.end(), positions);
+  }
+  return HALF_SUCCESS;
+}
+
+int half_get_system_info(half_handle handle, int* nions, int* ntypes, int grid[3], double lattice[9], double* volume,
+                         char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nions) *nions = ctx->crystal.nions();
+  if (ntypes) *ntypes = ctx->crystal.ntypes();
+  if (grid) for (int i = 0; i < 3; ++i) grid[i] = ctx->charge.shape[i];
+  if (lattice) for (int i = 0; i < 9; ++i) lattice[i] = ctx->crystal.lattice[i];
+  if (volume) *volume = ctx->crystal.volume();
+  return HALF_SUCCESS;
+}
+
+int half_get_basis_size(half_handle handle, const double kpoint[3], int64_t* npw, char* error, int cap) {
+  clear_error(error, cap);
+  if (npw) *npw = 0;
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  return guarded(error, cap, [&]() -> int {
+    if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
+    Basis b = build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoint);
+    if (npw) *npw = b.npw();
+    return HALF_SUCCESS;
+  });
+}
+
+int half_get_basis(half_handle handle, const double kpoint[3], int64_t capacity, int32_t* gvec, double* kinetic,
+                   char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  return guarded(error, cap, [&]() -> int {
+    if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
+    Basis b = build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoint);
+    if (capacity < b.npw()) fail(kCapacity, "basis output capacity is too small");
+    for (long long i = 0; i < b.npw(); ++i) {
+      if (gvec) for (int j = 0; j < 3; ++j) gvec[3 * i + j] = b.gvec[3 * i + j];
+      if (kinetic) kinetic[i] = b.kinetic[i];
+    }
+    return HALF_SUCCESS;
+  });
+}
+
+int half_assemble_hs(half_handle handle, const double kpoint[3], int64_t ld, HALF_C128* h, HALF_C128* s, char* error,
+                     int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!h || !s) { export_error("H and S output pointers are required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  return guarded(error, cap, [&]() -> int {
+    if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
+    auto ks = prepare_operator(*ctx, kpoint, true, false);
+    long long n = ks->basis.npw();
+    if (ld < n) fail(kCapacity, "matrix leading dimension is too small");
+    DeviceBuffer<double2> dh((size_t)n * n), ds((size_t)n * n);
+    assemble_dense(*ctx, *ks, dh.get(), ds.get());
+    cudaStream_t st = ctx->rt->stream;
+    HALF_CUDA(cudaMemcpy2DAsync(h, ld * sizeof(double2), dh.get(), n * sizeof(double2), n * sizeof(double2), n,
+                                cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaMemcpy2DAsync(s, ld * sizeof(double2), ds.get(), n * sizeof(double2), n * sizeof(double2), n,
+                                cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaStreamSynchronize(st));
+    return HALF_SUCCESS;
+  });
+}
+
+int half_apply_hs(half_handle handle, const double kpoint[3], int nstates, int64_t ld, const HALF_C128* psi,
+                  HALF_C128* hpsi, HALF_C128* spsi, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nstates < 1 || !psi || !hpsi || !spsi) { export_error("invalid state block arguments", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  return guarded(error, cap, [&]() -> int {
+    if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
+    bool fp32 = ctx->acc.precision == kMixed;
+    auto ks = prepare_operator(*ctx, kpoint, true, fp32);
+    long long n = ks->basis.npw();
+    if (ld < n) fail(kCapacity, "state leading dimension is too small");
+    cudaStream_t st = ctx->rt->stream;
+    DeviceBuffer<double2> x((size_t)n * nstates), hx((size_t)n * nstates), sx((size_t)n * nstates);
+    HALF_CUDA(cudaMemcpy2DAsync(x.get(), n * sizeof(double2), psi, ld * sizeof(double2), n * sizeof(double2), nstates,
+                                cudaMemcpyHostToDevice, st));
+    apply_hs<double>(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
+    HALF_CUDA(cudaMemcpy2DAsync(hpsi, ld * sizeof(double2), hx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
+                                cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaMemcpy2DAsync(spsi, ld * sizeof(double2), sx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
+                                cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaStreamSynchronize(st));
+    return HALF_SUCCESS;
+  });
+}
+
+int half_solve_kpoint(half_handle handle, const double kpoint[3], int nbands, double* eigenvalues, HALF_C128* vectors,
+                      int64_t ld, double* overlap_min, double* overlap_max, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nbands < 1) { export_error("band count must be positive", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  return guarded(error, cap, [&]() -> int {
+    SolveOutput out;
+    std::unique_ptr<KOperatorSet> ks;
+    solve_one(*ctx, kpoint, nbands, false, out, &ks);
+    long long n = ks->basis.npw();
+    if (vectors && ld < n) fail(kCapacity, "eigenvector leading dimension is too small");
+    if (eigenvalues) std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues);
+    if (overlap_min) *overlap_min = out.overlap_min;
+    if (overlap_max) *overlap_max = out.overlap_max;
+    if (vectors) {
+      cudaStream_t st = ctx->rt->stream;
+      HALF_CUDA(cudaMemcpy2DAsync(vectors, ld * sizeof(double2), out.dvectors.get(), n * sizeof(double2),
+                                  n * sizeof(double2), nbands, cudaMemcpyDeviceToHost, st));
+      HALF_CUDA(cudaStreamSynchronize(st));
+    }
+    return HALF_SUCCESS;
+  });
+}
+
+namespace {
+int g_hash(int32_t gx, int32_t gy, int32_t gz, int table_size) {   // src/half_c_api.F90:590-597 (0-based)
+  long long v = (long long)gx * 73856093LL + (long long)gy * 19349663LL + (long long)gz * 83492791LL;
+  long long m = v % table_size;
+  if (m < 0) m += table_size;
+  return int(m);
+}
+}  // namespace
+
+int half_solve_kpoint_mapped(half_handle handle, const double kpoint[3], int nbands, int64_t host_npw,
+                             const int32_t* host_gvec, double* eigenvalues, HALF_C128* vectors, int64_t ld,
+                             double* overlap_min, double* overlap_max, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nbands < 1 || host_npw < 1 || ld < host_npw || !vectors || !host_gvec) {
+    export_error("invalid mapped-solve band count, basis size, leading dimension, or output pointer", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    SolveOutput out;
+    std::unique_ptr<KOperatorSet> ks;
+    solve_one(*ctx, kpoint, nbands, true, out, &ks);
+    const Basis& b = ks->basis;
+    long long n = b.npw();
+    if (host_npw != n) fail(kInvalidArgument, "host and HALF plane-wave bases have different sizes");
+    int table_size = 1;
+    while (table_size < 2 * n) table_size *= 2;
+    std::vector<int> table(table_size, -1);
+    for (long long hi = 0; hi < n; ++hi) {
+      int p = g_hash(host_gvec[3 * hi], host_gvec[3 * hi + 1], host_gvec[3 * hi + 2], table_size);
+      while (table[p] >= 0) {
+        int i = table[p];
+        if (host_gvec[3 * i] == host_gvec[3 * hi] && host_gvec[3 * i + 1] == host_gvec[3 * hi + 1] &&
+            host_gvec[3 * i + 2] == host_gvec[3 * hi + 2])
+          fail(kInvalidArgument, "host G-vector list contains a duplicate");
+        p = (p + 1) % table_size;
+      }
+      table[p] = int(hi);
+    }
+    std::vector<long long> perm(n);
+    for (long long i = 0; i < n; ++i) {
+      int p = g_hash(b.gvec[3 * i], b.gvec[3 * i + 1], b.gvec[3 * i + 2], table_size), hit = -1;
+      while (table[p] >= 0) {
+        int j = table[p];
+        if (host_gvec[3 * j] == b.gvec[3 * i] && host_gvec[3 * j + 1] == b.gvec[3 * i + 1] &&
+            host_gvec[3 * j + 2] == b.gvec[3 * i + 2]) { hit = j; break; }
+        p = (p + 1) % table_size;
+      }
+      if (hit < 0) fail(kInvalidArgument, "host and HALF plane-wave bases contain different G vectors");
+      perm[i] = hit;
+    }
+    double* dst = reinterpret_cast<double*>(vectors);
+    std::fill(dst, dst + 2 * ld * nbands, 0.0);
+    for (int bnd = 0; bnd < nbands; ++bnd)
+      for (long long i = 0; i < n; ++i) {
+        dst[2 * (bnd * ld + perm[i])] = out.vectors[2 * (bnd * n + i)];
+        dst[2 * (bnd * ld + perm[i]) + 1] = out.vectors[2 * (bnd * n + i) + 1];
+      }
+    if (eigenvalues) std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues);
+    if (overlap_min) *overlap_min = out.overlap_min;
+    if (overlap_max) *overlap_max = out.overlap_max;
+    return HALF_SUCCESS;
+  });
+}
+
+// ------------------------------------------------------------- extensions
+
+int half_set_acc_controls(half_handle handle, double tol, int max_iterations, int block_size, int precision,
+                          char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!(tol > 0) || !std::isfinite(tol) || max_iterations < 1 || block_size < 1 ||
+      (precision != HALF_PRECISION_FP64 && precision != HALF_PRECISION_MIXED)) {
+    export_error("invalid ACC solver controls", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  ctx->acc.tol = tol;
+  ctx->acc.max_iter = max_iterations;
+  ctx->acc.block = block_size;
+  ctx->acc.precision = precision;
+  return HALF_SUCCESS;
+}
+
+int half_get_last_solve_info(half_handle handle, half_solve_info_v1* info, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!info || info->struct_size < sizeof(half_solve_info_v1)) {
+    export_error("solve info structure is missing or too small", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  const SolveInfo& s = ctx->last;
+  info->iterations = s.iterations;
+  info->fp64_iterations = s.fp64_iterations;
+  info->converged = s.converged;
+  info->npw = s.npw;
+  info->operator_applications = s.operator_columns;
+  info->max_residual_eV = s.max_residual;
+  info->setup_ms = s.setup_ms;
+  info->solve_ms = s.solve_ms;
+  info->operator_ms = s.operator_ms;
+  std::memset(info->reserved, 0, sizeof(info->reserved));
+  return HALF_SUCCESS;
+}
+
+int half_solve_kpoints(half_handle handle, int nk, const double* kpoints, int nbands, double* eigenvalues, char* error,
+                       int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || nbands < 1 || !eigenvalues) {
+    export_error("invalid k-point batch arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    SolveInfo total;
+    for (int ik = 0; ik < nk; ++ik) {
+      SolveOutput out;
+      solve_one(*ctx, kpoints + 3 * ik, nbands, false, out);
+      std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues + (size_t)ik * nbands);
+      total.iterations += ctx->last.iterations;
+      total.fp64_iterations += ctx->last.fp64_iterations;
+      total.converged = (ik == 0 ? 1 : total.converged) & ctx->last.converged;
+      total.operator_columns += ctx->last.operator_columns;
+      total.max_residual = std::max(total.max_residual, ctx->last.max_residual);
+      total.setup_ms += ctx->last.setup_ms;
+      total.solve_ms += ctx->last.solve_ms;
+      total.operator_ms += ctx->last.operator_ms;
+      total.npw += ctx->last.npw;
+    }
+    ctx->last = total;
+    return HALF_SUCCESS;
+  });
+}
+
+int half_set_positions(half_handle handle, const double* positions, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!positions) { export_error("positions pointer is required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  return guarded(error, cap, [&]() -> int {
+    int n = ctx->crystal.nions();
+    for (int i = 0; i < 3 * n; ++i)
+      if (!std::isfinite(positions[i])) fail(kInvalidArgument, "positions must be finite");
+    ctx->crystal.positions.assign(positions, positions + 3 * n);
+    ctx->rebuild_dij();
+    return HALF_SUCCESS;
+  });
+}
+
+int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands, int64_t ld, const HALF_C128* vectors,
+                         const double* eigenvalues, const double* occupations, double kweight, double* forces,
+                         char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nbands < 1 || !vectors || !eigenvalues || !occupations || !forces) {
+    export_error("invalid force arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
+    auto ks = prepare_operator(*ctx, kpoint, true, false);
+    long long n = ks->basis.npw();
+    if (ld < n) fail(kCapacity, "eigenvector leading dimension is too small");
+    cudaStream_t st = ctx->rt->stream;
+    DeviceBuffer<double2> dv((size_t)n * nbands);
+    HALF_CUDA(cudaMemcpy2DAsync(dv.get(), n * sizeof(double2), vectors, ld * sizeof(double2), n * sizeof(double2),
+                                nbands, cudaMemcpyHostToDevice, st));
+    nonlocal_forces_device(*ctx, *ks, dv.get(), n, nbands, eigenvalues, occupations, kweight, forces);
+    return HALF_SUCCESS;
+  });
+}
+
+}  // extern "C"
+
+// occupations (src/half_energy.F90:41-120), shared with half_band_forces
+namespace hb {
+void compute_occupations(const std::vector<double>& eig, int nk, int nb, const double* w, double nelect, double sigma,
+                         int ismear, std::vector<double>& occ, double& mu, double& band, double& entropy);
+}
+
+extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoints, const double* kweights, int nbands,
+                                double nelect, double sigma, int ismear, double* forces, double* eig_out,
+                                double* occ_out, double* energies, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || !kweights || nbands < 1 || !forces || !(sigma >= 0) || (ismear != -1 && ismear != 0)) {
+    export_error("invalid band-force arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    std::vector<SolveOutput> outs(nk);
+    std::vector<double> eig((size_t)nk * nbands);
+    for (int ik = 0; ik < nk; ++ik) {
+      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik]);
+      std::copy(outs[ik].eigenvalues.begin(), outs[ik].eigenvalues.end(), eig.begin() + (size_t)ik * nbands);
+    }
+    std::vector<double> occ;
+    double mu = 0, band = 0, entropy = 0;
+    compute_occupations(eig, nk, nbands, kweights, nelect, sigma, ismear, occ, mu, band, entropy);
+    int nions = ctx->crystal.nions();
+    std::fill(forces, forces + 3 * nions, 0.0);
+    for (int ik = 0; ik < nk; ++ik) {
+      auto ks = prepare_operator(*ctx, kpoints + 3 * ik, true, false);
+      nonlocal_forces_device(*ctx, *ks, outs[ik].dvectors.get(), ks->basis.npw(), nbands, eig.data() + (size_t)ik * nbands,
+                             occ.data() + (size_t)ik * nbands, kweights[ik], forces);
+    }
+    if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
+    if (occ_out) std::copy(occ.begin(), occ.end(), occ_out);
+    if (energies) { energies[0] = band; energies[1] = entropy; energies[2] = mu; }
+    return HALF_SUCCESS;
+  });
+}

@@ -1,0 +1,41 @@
+// Thin typed wrappers over the cuBLAS / cuSOLVER calls the solvers make.
+// Complex FP64 maps to Z routines; complex FP32 to C routines, which the
+// runtime routes to the BF16x9 tensor-core emulation when cuBLAS offers it.
+#pragma once
+
+#include "context.h"
+
+namespace hb {
+
+inline void gemm(Runtime& rt, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, double2 alpha,
+                 const double2* A, long long lda, const double2* B, long long ldb, double2 beta, double2* C,
+                 long long ldc) {
+  if (m <= 0 || n <= 0) return;
+  cublas_check(cublasZgemm(rt.blas, ta, tb, m, n, k, reinterpret_cast<const cuDoubleComplex*>(&alpha),
+                           reinterpret_cast<const cuDoubleComplex*>(A), int(lda),
+                           reinterpret_cast<const cuDoubleComplex*>(B), int(ldb),
+                           reinterpret_cast<const cuDoubleComplex*>(&beta), reinterpret_cast<cuDoubleComplex*>(C),
+                           int(ldc)),
+               "zgemm");
+}
+
+inline void gemm(Runtime& rt, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, float2 alpha,
+                 const float2* A, long long lda, const float2* B, long long ldb, float2 beta, float2* C,
+                 long long ldc) {
+  if (m <= 0 || n <= 0) return;
+  cublas_check(cublasCgemm(rt.blas, ta, tb, m, n, k, reinterpret_cast<const cuComplex*>(&alpha),
+                           reinterpret_cast<const cuComplex*>(A), int(lda), reinterpret_cast<const cuComplex*>(B),
+                           int(ldb), reinterpret_cast<const cuComplex*>(&beta), reinterpret_cast<cuComplex*>(C),
+                           int(ldc)),
+               "cgemm");
+}
+
+template <typename R>
+inline cplx_t<R> cval(double x, double y = 0) {
+  cplx_t<R> c;
+  c.x = R(x);
+  c.y = R(y);
+  return c;
+}
+
+}  // namespace hb

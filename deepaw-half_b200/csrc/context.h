@@ -1,0 +1,136 @@
+// Library context and the per-k operator objects of the B200 path.
+#pragma once
+
+#include <array>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "fft.cuh"
+#include "io.h"
+#include "radial.h"
+
+namespace hb {
+
+enum Precision : int { kFP64 = 0, kMixed = 1 };
+
+// ACC controls; the defaults are the reference's (src/half_cuda_iterative_solver.cuf:113-118).
+struct AccControls {
+  double tol = 1.0e-4;
+  int max_iter = 40;
+  int block = 16;
+  int precision = kFP64;
+};
+
+struct SolveInfo {
+  int iterations = 0, fp64_iterations = 0, converged = 0;
+  long long npw = 0, operator_columns = 0;
+  double max_residual = 0, setup_ms = 0, solve_ms = 0, operator_ms = 0;
+};
+
+// Per-stream library handles.
+struct Runtime {
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  bool bf16x9 = false;   // cuBLAS offers FP32 emulation on BF16 tensor cores
+  Runtime();
+  ~Runtime();
+  Runtime(const Runtime&) = delete;
+  Runtime& operator=(const Runtime&) = delete;
+};
+
+// Plane-wave basis (src/half_basis.F90:9-55); fft_index is 0-based C order.
+struct Basis {
+  std::array<int, 3> shape{};
+  std::array<double, 3> kpoint{};
+  std::vector<int> gvec;          // npw*3
+  std::vector<double> qvec;       // npw*3, A^-1
+  std::vector<double> kinetic;    // npw, eV
+  std::vector<long long> fft_index;
+  long long npw() const { return (long long)kinetic.size(); }
+};
+Basis build_basis(const Crystal& c, const std::array<int, 3>& shape, double encut, const double k[3]);
+
+// Device copy of everything the projector/D stage needs for one species.
+struct SpeciesDevice {
+  int natoms = 0, nlm = 0, first_ion = 0, nchan = 0;
+  std::vector<int> lps;
+  QdepTables tables;                   // host tables (QDEP)
+  DeviceBuffer<double> dij;            // natoms * nlm * nlm, row-major per atom
+  DeviceBuffer<double> ddij;           // natoms * 3 * nlm * nlm
+  std::vector<double> dij_host;        // mirror of dij
+  DeviceBuffer<double> qij;            // nlm * nlm
+  std::vector<double> qij_host;
+  double pspnl_gmax = 0;
+  std::vector<double> radial_y, radial_m2;   // [channel][100]
+};
+
+struct Context {
+  Crystal crystal;
+  ChargeGrid charge;
+  std::vector<Potcar> pots;
+  double encut = 0;
+  bool use_pbe = true, use_uspp = true;
+  int backend = 2, solver = 1;
+  AccControls acc;
+  SolveInfo last;
+  // request geometry (deep copy, src/half_library.F90:227-247)
+  bool has_request_geometry = false;
+  int request_nions = 0, request_ntypes = 0;
+  std::array<int, 3> request_grid{};
+  std::array<double, 9> request_lattice{};
+  std::vector<int> request_species;
+  std::vector<double> request_positions;
+
+  std::unique_ptr<Runtime> rt;
+  DeviceBuffer<double> veff;           // C order, eV
+  std::vector<SpeciesDevice> species;
+
+  void initialize();                   // Veff + QDEP on the device
+  void rebuild_dij();                  // QDEP at fixed Veff (positions changed)
+  long long nr() const { return (long long)charge.shape[0] * charge.shape[1] * charge.shape[2]; }
+};
+
+// ----------------------------------------------------------------- set-up
+void build_veff_device(Context& ctx);                 // setup.cu
+void build_dij_device(Context& ctx, bool gradient);   // setup.cu
+void fft3d_inplace(double2* data, const std::array<int, 3>& shape, int sign, cudaStream_t s);
+
+// ----------------------------------------------------------------- operator
+template <typename R>
+struct KOperator;   // hs.cu
+
+struct KOperatorSet {
+  Basis basis;
+  int np = 0;                                 // projector columns (all species)
+  std::unique_ptr<KOperator<double>> op64;
+  std::unique_ptr<KOperator<float>> op32;
+  DeviceBuffer<double> qvec;                  // npw*3 (forces)
+  ~KOperatorSet();
+};
+
+std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, const double k[3], bool fp64, bool fp32);
+
+// H/S application on device blocks (column-major, leading dimension ld).
+template <typename R>
+void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx,
+              cplx_t<R>* sx, int chunk);
+
+// ----------------------------------------------------------------- solvers
+struct SolveOutput {
+  std::vector<double> eigenvalues;
+  std::vector<double> vectors;       // interleaved complex, npw x nbands (optional)
+  double overlap_min = -1, overlap_max = -1;
+  DeviceBuffer<double2> dvectors;    // device copy (kept for forces)
+};
+void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out);
+void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, bool want_vectors, SolveOutput& out);
+void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s);   // device N x N
+
+// ----------------------------------------------------------------- forces
+void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec, long long ld, int nb,
+                            const double* eig, const double* occ, double kweight, double* forces_host);
+
+}  // namespace hb

@@ -1,0 +1,478 @@
+// The matrix-free MIMIC_US H/S operator of one k point.
+//
+// Reference: apply_hs_operator_cuda (src/half_cuda_assembly.cuf:468-519)
+// scatters each band into a zeroed N_r box, runs one cuFFT per band inverse,
+// multiplies by Veff/N_r, one cuFFT per band forward, gathers and adds T psi,
+// then per species runs three ZGEMMs around a D/Q mixing kernel.
+//
+// B200 design: the local part is three fused kernels over x-planes of the box
+// that never materialise empty data.  Planes are indexed by g1 in the
+// sphere's x-extent only (about 40% of the box); within a plane only the rows
+// that hold sphere points are transformed along z.
+//   K1  sphere -> planes: scatter band points straight into the transform's
+//       digit-reversed slots, inverse z FFT on occupied rows, inverse y FFT
+//       on all columns, one coalesced plane store;
+//   K2  x lines: gather the occupied x slots, inverse x FFT, multiply by
+//       Veff/N_r, forward x FFT, store the occupied slots back;
+//   K3  planes -> sphere: forward y FFT, forward z FFT on occupied rows,
+//       gather sphere points, H psi = . + T psi, S psi = psi.
+// Bands go through in chunks (the ACC block size) so the plane buffer of a
+// chunk stays resident in the 126 MB L2 between the three kernels.  The
+// projector part is one GEMM B^H X over all species and bands, a D/Q mixing
+// kernel and two GEMMs accumulating into H X and S X.
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+#include "blas.h"
+#include "context.h"
+
+namespace hb {
+
+template <typename R>
+struct KOperator {
+  using C = cplx_t<R>;
+  int npw = 0, n1 = 0, n2 = 0, n3 = 0, g1min = 0, nplanes = 0, np = 0, max_rows = 0;
+  AxisPlan ax, ay, az;
+  DeviceBuffer<int> plane_start, spos, row_start, row_list, plane_xpos;
+  DeviceBuffer<R> veff;      // Veff / N_r, C order
+  DeviceBuffer<R> kinetic;
+  DeviceBuffer<C> work;      // chunk x nplanes x n2 x n3
+  int work_chunk = 0;
+  DeviceBuffer<C> B;         // npw x np, column-major
+  DeviceBuffer<R> dall, qall;            // D per atom, Q per species
+  DeviceBuffer<int> col_base, col_a, col_nlm, col_dofs, col_qofs;
+  DeviceBuffer<C> coeff, dy, qy;
+  int ws_cols = 0;
+};
+
+KOperatorSet::~KOperatorSet() = default;
+
+namespace {
+
+constexpr int kXTile = 16;
+
+template <typename C>
+__device__ __forceinline__ C czero() { C c; c.x = 0; c.y = 0; return c; }
+
+template <typename R>
+__global__ void __launch_bounds__(512) k1_sphere_to_planes(const cplx_t<R>* __restrict__ psi, long long ld, int b0,
+                                                           int n2, int n3, int nplanes, const int* __restrict__ plane_start,
+                                                           const int* __restrict__ spos, const int* __restrict__ row_start,
+                                                           const int* __restrict__ row_list, AxisPlan ay, AxisPlan az,
+                                                           cplx_t<R>* __restrict__ work) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* twy = reinterpret_cast<C*>(smem_raw);
+  C* twz = twy + kMaxFFT;
+  C* plane = twz + kMaxFFT;
+  int* rows = reinterpret_cast<int*>(plane + n2 * n3);
+  const int j = blockIdx.x, b = blockIdx.y;
+  fill_twiddles(twy, n2);
+  fill_twiddles(twz, n3);
+  const int npl = n2 * n3;
+  for (int t = threadIdx.x; t < npl; t += blockDim.x) plane[t] = czero<C>();
+  const int r0 = row_start[j], nrows = row_start[j + 1] - r0;
+  for (int t = threadIdx.x; t < nrows; t += blockDim.x) rows[t] = row_list[r0 + t];
+  __syncthreads();
+  const C* col = psi + (long long)(b0 + b) * ld;
+  const int p0 = plane_start[j], p1 = plane_start[j + 1];
+  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) plane[spos[p]] = col[p];
+  __syncthreads();
+  fft_pencils<true, C, R>(plane, nrows, n3, 1, az.plan, twz, +1, rows);
+  fft_pencils<true, C, R>(plane, n3, 1, n3, ay.plan, twy, +1);
+  C* dst = work + ((long long)b * nplanes + j) * npl;
+  for (int t = threadIdx.x; t < npl; t += blockDim.x) dst[t] = plane[t];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k2_xlines(cplx_t<R>* __restrict__ work, int n1, int n2, int n3, int nplanes,
+                                                 const int* __restrict__ plane_xpos, AxisPlan ax,
+                                                 const R* __restrict__ veff) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* X = tw + kMaxFFT;                                 // [i1][tz]
+  int* xpos = reinterpret_cast<int*>(X + n1 * kXTile);
+  const int tiles = (n3 + kXTile - 1) / kXTile;
+  const int i2 = blockIdx.x / tiles, z0 = (blockIdx.x - i2 * tiles) * kXTile;
+  const int nz = min(kXTile, n3 - z0);
+  const int b = blockIdx.y;
+  fill_twiddles(tw, n1);
+  for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) X[t] = czero<C>();
+  for (int t = threadIdx.x; t < nplanes; t += blockDim.x) xpos[t] = plane_xpos[t];
+  __syncthreads();
+  const long long npl = (long long)n2 * n3;
+  C* base = work + (long long)b * nplanes * npl + (long long)i2 * n3 + z0;
+  for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
+    int jj = t / kXTile, c = t - jj * kXTile;
+    if (c < nz) X[xpos[jj] * kXTile + c] = base[jj * npl + c];
+  }
+  __syncthreads();
+  fft_pencils<true, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, +1);
+  for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) {
+    int i1 = t / kXTile, c = t - i1 * kXTile;
+    if (c < nz) X[t] = cscale(X[t], veff[((long long)i1 * n2 + i2) * n3 + z0 + c]);
+  }
+  __syncthreads();
+  fft_pencils<false, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, -1);
+  for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
+    int jj = t / kXTile, c = t - jj * kXTile;
+    if (c < nz) base[jj * npl + c] = X[xpos[jj] * kXTile + c];
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(512) k3_planes_to_sphere(const cplx_t<R>* __restrict__ work, int n2, int n3,
+                                                           int nplanes, const int* __restrict__ plane_start,
+                                                           const int* __restrict__ spos, const int* __restrict__ row_start,
+                                                           const int* __restrict__ row_list, AxisPlan ay, AxisPlan az,
+                                                           const cplx_t<R>* __restrict__ psi, long long ld, int b0,
+                                                           const R* __restrict__ kinetic, cplx_t<R>* __restrict__ hpsi,
+                                                           cplx_t<R>* __restrict__ spsi) {
+  using C = cplx_t<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* twy = reinterpret_cast<C*>(smem_raw);
+  C* twz = twy + kMaxFFT;
+  C* plane = twz + kMaxFFT;
+  int* rows = reinterpret_cast<int*>(plane + n2 * n3);
+  const int j = blockIdx.x, b = blockIdx.y;
+  fill_twiddles(twy, n2);
+  fill_twiddles(twz, n3);
+  const int npl = n2 * n3;
+  const C* src = work + ((long long)b * nplanes + j) * npl;
+  for (int t = threadIdx.x; t < npl; t += blockDim.x) plane[t] = src[t];
+  const int r0 = row_start[j], nrows = row_start[j + 1] - r0;
+  for (int t = threadIdx.x; t < nrows; t += blockDim.x) rows[t] = row_list[r0 + t];
+  __syncthreads();
+  fft_pencils<false, C, R>(plane, n3, 1, n3, ay.plan, twy, -1);
+  fft_pencils<false, C, R>(plane, nrows, n3, 1, az.plan, twz, -1, rows);
+  const long long off = (long long)(b0 + b) * ld;
+  const int p0 = plane_start[j], p1 = plane_start[j + 1];
+  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+    C x = psi[off + p];
+    C h = plane[spos[p]];
+    R kin = kinetic[p];
+    h.x += kin * x.x;
+    h.y += kin * x.y;
+    hpsi[off + p] = h;
+    spsi[off + p] = x;
+  }
+}
+
+// dy[:,b] = blockdiag(D_atom) coeff[:,b], qy[:,b] = blockdiag(Q_species) coeff[:,b]
+// (src/half_cuda_assembly.cuf:220-237)
+template <typename R>
+__global__ void mix_kernel(const cplx_t<R>* __restrict__ coeff, int np, int nb, const int* __restrict__ col_base,
+                           const int* __restrict__ col_a, const int* __restrict__ col_nlm,
+                           const int* __restrict__ col_dofs, const int* __restrict__ col_qofs,
+                           const R* __restrict__ dall, const R* __restrict__ qall, cplx_t<R>* __restrict__ dy,
+                           cplx_t<R>* __restrict__ qy) {
+  using C = cplx_t<R>;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)np * nb) return;
+  int p = int(idx % np);
+  long long b = idx / np;
+  const int base = col_base[p], a = col_a[p], nlm = col_nlm[p];
+  const R* drow = dall + col_dofs[p] + a * nlm;
+  const R* qrow = qall + col_qofs[p] + a * nlm;
+  const C* c = coeff + b * np + base;
+  C zd = czero<C>(), zq = czero<C>();
+  for (int k = 0; k < nlm; ++k) {
+    C v = c[k];
+    zd.x += drow[k] * v.x; zd.y += drow[k] * v.y;
+    zq.x += qrow[k] * v.x; zq.y += qrow[k] * v.y;
+  }
+  dy[idx] = zd;
+  qy[idx] = zq;
+}
+
+struct ProjCol {
+  int chan;      // global channel index into the radial tables
+  int l, m;
+  int ion;
+  double gmax;
+};
+
+// B[g, p] = Omega^-1/2 (-i)^l beta_l(|q|) Y_lm(q^) exp(-i q.R)   (src/half_paw.F90:52-65)
+__global__ void projector_kernel(double2* __restrict__ B, int npw, const double* __restrict__ q,
+                                 const ProjCol* __restrict__ cols, const double* __restrict__ ry,
+                                 const double* __restrict__ rm2, const double* __restrict__ pos, double pref) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int p = blockIdx.y;
+  if (g >= npw) return;
+  const ProjCol col = cols[p];
+  double qx = q[3 * g], qy = q[3 * g + 1], qz = q[3 * g + 2];
+  double qn = sqrt(qx * qx + qy * qy + qz * qz);
+  double theta = 0, phi = 0;
+  if (qn > 1.0e-10) {
+    theta = acos(fmax(-1.0, fmin(1.0, qz / qn)));
+    phi = atan2(qy, qx);
+  }
+  double rval = spline_eval(ry + col.chan * 100, rm2 + col.chan * 100, 100, col.gmax, qn);
+  if (qn > 0.99 * col.gmax) rval = 0;
+  double ylm = real_ylm(col.l, col.m, cos(theta), phi);
+  double ph = qx * pos[3 * col.ion] + qy * pos[3 * col.ion + 1] + qz * pos[3 * col.ion + 2];
+  double s, c;
+  sincos(ph, &s, &c);
+  double amp = pref * rval * ylm;
+  // (-i)^l * (cos - i sin)
+  double re = amp * c, im = -amp * s, tr, ti;
+  switch (col.l & 3) {
+    case 0: tr = re; ti = im; break;
+    case 1: tr = im; ti = -re; break;
+    case 2: tr = -re; ti = -im; break;
+    default: tr = -im; ti = re; break;
+  }
+  B[(long long)p * npw + g] = make_double2(tr, ti);
+}
+
+__global__ void to_float_kernel(const double2* __restrict__ in, float2* __restrict__ out, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_float2(float(in[i].x), float(in[i].y));
+}
+
+template <typename R>
+__global__ void scale_copy_kernel(const double* __restrict__ in, R* __restrict__ out, long long n, double s) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = R(in[i] * s);
+}
+
+template <typename R>
+size_t plane_smem(int n2, int n3) {
+  return (2 * kMaxFFT + size_t(n2) * n3) * sizeof(cplx_t<R>) + size_t(n2) * sizeof(int);
+}
+template <typename R>
+size_t xline_smem(int n1, int nplanes) {
+  return (kMaxFFT + size_t(n1) * kXTile) * sizeof(cplx_t<R>) + size_t(nplanes) * sizeof(int);
+}
+
+struct HostGeom {
+  int g1min = 0, nplanes = 0, max_rows = 0;
+  std::vector<int> plane_start, spos, row_start, row_list, plane_xpos;
+};
+
+HostGeom plane_geometry(const Basis& b, const AxisPlan& ax, const AxisPlan& ay, const AxisPlan& az) {
+  HostGeom h;
+  const int n1 = b.shape[0], n2 = b.shape[1], n3 = b.shape[2];
+  const long long npw = b.npw();
+  int g1min = b.gvec[0], g1max = b.gvec[3 * (npw - 1)];
+  h.g1min = g1min;
+  h.nplanes = g1max - g1min + 1;
+  if (h.nplanes > n1) fail(kInternal, "sphere x-extent exceeds the FFT box");
+  h.plane_start.assign(h.nplanes + 1, 0);
+  h.spos.resize(npw);
+  long long p = 0;
+  for (int j = 0; j < h.nplanes; ++j) {
+    h.plane_start[j] = int(p);
+    h.row_start.push_back(int(h.row_list.size()));
+    int last_i2 = -1;
+    while (p < npw && b.gvec[3 * p] == g1min + j) {
+      int i2 = ((b.gvec[3 * p + 1] % n2) + n2) % n2, i3 = ((b.gvec[3 * p + 2] % n3) + n3) % n3;
+      int row = ay.pos[i2];
+      if (i2 != last_i2) { h.row_list.push_back(row); last_i2 = i2; }
+      h.spos[p] = row * n3 + az.pos[i3];
+      ++p;
+    }
+    int i1 = (((g1min + j) % n1) + n1) % n1;
+    h.plane_xpos.push_back(ax.pos[i1]);
+  }
+  h.plane_start[h.nplanes] = int(p);
+  h.row_start.push_back(int(h.row_list.size()));
+  for (int j = 0; j < h.nplanes; ++j) h.max_rows = std::max(h.max_rows, h.row_start[j + 1] - h.row_start[j]);
+  if (p != npw) fail(kInternal, "basis is not ordered by g1");
+  return h;
+}
+
+template <typename R>
+void fill_operator(Context& ctx, const Basis& basis, const HostGeom& hg, const DeviceBuffer<double2>& B64, int np,
+                   const std::vector<int>& cb, const std::vector<int>& ca, const std::vector<int>& cn,
+                   const std::vector<int>& cd, const std::vector<int>& cq, KOperator<R>& op) {
+  cudaStream_t s = ctx.rt->stream;
+  op.npw = int(basis.npw());
+  op.n1 = basis.shape[0]; op.n2 = basis.shape[1]; op.n3 = basis.shape[2];
+  op.ax = make_axis_plan(op.n1); op.ay = make_axis_plan(op.n2); op.az = make_axis_plan(op.n3);
+  op.g1min = hg.g1min; op.nplanes = hg.nplanes; op.max_rows = hg.max_rows; op.np = np;
+  if (plane_smem<R>(op.n2, op.n3) > 227 * 1024)
+    fail(kUnavailable, "FFT plane " + std::to_string(op.n2) + "x" + std::to_string(op.n3) +
+                           " exceeds the shared-memory capacity of one CTA at this precision");
+  op.plane_start.upload(hg.plane_start, s);
+  op.spos.upload(hg.spos, s);
+  op.row_start.upload(hg.row_start, s);
+  op.row_list.upload(hg.row_list, s);
+  op.plane_xpos.upload(hg.plane_xpos, s);
+  const long long nr = ctx.nr();
+  op.veff.resize(nr);
+  scale_copy_kernel<R><<<ceil_div(nr, 256), 256, 0, s>>>(ctx.veff.get(), op.veff.get(), nr, 1.0 / double(nr));
+  DeviceBuffer<double> kin;
+  kin.upload(basis.kinetic, s);
+  op.kinetic.resize(basis.npw());
+  scale_copy_kernel<R><<<ceil_div(basis.npw(), 256), 256, 0, s>>>(kin.get(), op.kinetic.get(), basis.npw(), 1.0);
+  if constexpr (sizeof(R) == 8) {
+    op.B.resize(B64.size());
+    HALF_CUDA(cudaMemcpyAsync(op.B.get(), B64.get(), B64.size() * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  } else {
+    op.B.resize(B64.size());
+    to_float_kernel<<<ceil_div((long long)B64.size(), 256), 256, 0, s>>>(B64.get(), op.B.get(), (long long)B64.size());
+  }
+  std::vector<double> dall, qall;
+  for (auto& sp : ctx.species) {
+    dall.insert(dall.end(), sp.dij_host.begin(), sp.dij_host.end());
+    qall.insert(qall.end(), sp.qij_host.begin(), sp.qij_host.end());
+  }
+  DeviceBuffer<double> dd, dq;
+  dd.upload(dall, s);
+  dq.upload(qall, s);
+  op.dall.resize(dall.size());
+  op.qall.resize(qall.size());
+  scale_copy_kernel<R><<<ceil_div((long long)dall.size(), 256), 256, 0, s>>>(dd.get(), op.dall.get(), (long long)dall.size(), 1.0);
+  scale_copy_kernel<R><<<ceil_div((long long)qall.size(), 256), 256, 0, s>>>(dq.get(), op.qall.get(), (long long)qall.size(), 1.0);
+  op.col_base.upload(cb, s);
+  op.col_a.upload(ca, s);
+  op.col_nlm.upload(cn, s);
+  op.col_dofs.upload(cd, s);
+  op.col_qofs.upload(cq, s);
+  HALF_LAUNCH("operator tables");
+  HALF_CUDA(cudaStreamSynchronize(s));
+  HALF_CUDA(cudaFuncSetAttribute(k1_sphere_to_planes<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(plane_smem<R>(op.n2, op.n3))));
+  HALF_CUDA(cudaFuncSetAttribute(k3_planes_to_sphere<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(plane_smem<R>(op.n2, op.n3))));
+  HALF_CUDA(cudaFuncSetAttribute(k2_xlines<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(xline_smem<R>(op.n1, op.nplanes))));
+}
+
+}  // namespace
+
+std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, const double k[3], bool fp64, bool fp32) {
+  auto ks = std::make_unique<KOperatorSet>();
+  ks->basis = build_basis(ctx.crystal, ctx.charge.shape, ctx.encut, k);
+  const Basis& basis = ks->basis;
+  const int npw = int(basis.npw());
+  if (npw < 1) fail(kInvalidArgument, "empty plane-wave basis");
+  cudaStream_t s = ctx.rt->stream;
+  AxisPlan ax = make_axis_plan(basis.shape[0]), ay = make_axis_plan(basis.shape[1]), az = make_axis_plan(basis.shape[2]);
+  HostGeom hg = plane_geometry(basis, ax, ay, az);
+  // projector columns: species-major, atom-major, then (channel, m)
+  std::vector<ProjCol> cols;
+  std::vector<int> cb, ca, cn, cd, cq;
+  std::vector<double> ry, rm2, pos;
+  int chan0 = 0, dofs = 0, qofs = 0, col0 = 0;
+  for (auto& sp : ctx.species) {
+    for (int a = 0; a < sp.natoms; ++a) {
+      int ilm = 0;
+      for (int c = 0; c < sp.nchan; ++c) {
+        int l = sp.lps[c];
+        for (int m = -l; m <= l; ++m, ++ilm) {
+          cols.push_back({chan0 + c, l, m, sp.first_ion + a, sp.pspnl_gmax});
+          cb.push_back(col0 + a * sp.nlm);
+          ca.push_back(ilm);
+          cn.push_back(sp.nlm);
+          cd.push_back(dofs + a * sp.nlm * sp.nlm);
+          cq.push_back(qofs);
+        }
+      }
+    }
+    ry.insert(ry.end(), sp.radial_y.begin(), sp.radial_y.end());
+    rm2.insert(rm2.end(), sp.radial_m2.begin(), sp.radial_m2.end());
+    chan0 += sp.nchan;
+    dofs += sp.natoms * sp.nlm * sp.nlm;
+    qofs += sp.nlm * sp.nlm;
+    col0 += sp.natoms * sp.nlm;
+  }
+  for (int i = 0; i < ctx.crystal.nions(); ++i) {
+    auto r = ctx.crystal.cartesian(i);
+    pos.insert(pos.end(), r.begin(), r.end());
+  }
+  const int np = int(cols.size());
+  ks->np = np;
+  ks->qvec.upload(basis.qvec, s);
+  DeviceBuffer<ProjCol> dcols;
+  dcols.upload(cols, s);
+  DeviceBuffer<double> dry, drm2, dpos;
+  dry.upload(ry, s);
+  drm2.upload(rm2, s);
+  dpos.upload(pos, s);
+  DeviceBuffer<double2> B64((size_t)npw * np);
+  if (np > 0) {
+    projector_kernel<<<dim3(ceil_div(npw, 256), np), 256, 0, s>>>(B64.get(), npw, ks->qvec.get(), dcols.get(), dry.get(),
+                                                                   drm2.get(), dpos.get(), 1.0 / std::sqrt(ctx.crystal.volume()));
+    HALF_LAUNCH("projectors");
+  }
+  if (fp64) {
+    ks->op64 = std::make_unique<KOperator<double>>();
+    fill_operator<double>(ctx, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op64);
+  }
+  if (fp32) {
+    ks->op32 = std::make_unique<KOperator<float>>();
+    fill_operator<float>(ctx, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op32);
+  }
+  HALF_CUDA(cudaStreamSynchronize(s));
+  return ks;
+}
+
+template <typename R>
+KOperator<R>& pick(KOperatorSet& ks);
+template <>
+KOperator<double>& pick<double>(KOperatorSet& ks) {
+  if (!ks.op64) fail(kInternal, "FP64 operator not prepared");
+  return *ks.op64;
+}
+template <>
+KOperator<float>& pick<float>(KOperatorSet& ks) {
+  if (!ks.op32) fail(kInternal, "FP32 operator not prepared");
+  return *ks.op32;
+}
+
+template <typename R>
+void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx, cplx_t<R>* sx,
+              int chunk) {
+  using C = cplx_t<R>;
+  KOperator<R>& op = pick<R>(ks);
+  Runtime& rt = *ctx.rt;
+  cudaStream_t s = rt.stream;
+  if (nb <= 0) return;
+  chunk = std::max(1, std::min(chunk, nb));
+  if (op.work_chunk < chunk) {
+    op.work.resize((size_t)chunk * op.nplanes * op.n2 * op.n3);
+    op.work_chunk = chunk;
+  }
+  const size_t psm = plane_smem<R>(op.n2, op.n3), xsm = xline_smem<R>(op.n1, op.nplanes);
+  const int tiles = (op.n3 + kXTile - 1) / kXTile;
+  for (int b0 = 0; b0 < nb; b0 += chunk) {
+    int nbc = std::min(chunk, nb - b0);
+    k1_sphere_to_planes<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
+        x, ld, b0, op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(), op.row_list.get(),
+        op.ay, op.az, op.work.get());
+    k2_xlines<R><<<dim3(op.n2 * tiles, nbc), 256, xsm, s>>>(op.work.get(), op.n1, op.n2, op.n3, op.nplanes,
+                                                           op.plane_xpos.get(), op.ax, op.veff.get());
+    k3_planes_to_sphere<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
+        op.work.get(), op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(),
+        op.row_list.get(), op.ay, op.az, x, ld, b0, op.kinetic.get(), hx, sx);
+  }
+  HALF_LAUNCH("local operator");
+  if (op.np == 0) return;
+  if (op.ws_cols < nb) {
+    op.coeff.resize((size_t)op.np * nb);
+    op.dy.resize((size_t)op.np * nb);
+    op.qy.resize((size_t)op.np * nb);
+    op.ws_cols = nb;
+  }
+  const C one = cval<R>(1.0), zero = cval<R>(0.0);
+  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, op.np, nb, op.npw, one, op.B.get(), op.npw, x, ld, zero, op.coeff.get(), op.np);
+  mix_kernel<R><<<ceil_div((long long)op.np * nb, 256), 256, 0, s>>>(op.coeff.get(), op.np, nb, op.col_base.get(),
+                                                                     op.col_a.get(), op.col_nlm.get(), op.col_dofs.get(),
+                                                                     op.col_qofs.get(), op.dall.get(), op.qall.get(),
+                                                                     op.dy.get(), op.qy.get());
+  HALF_LAUNCH("mix");
+  gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.dy.get(), op.np, one, hx, ld);
+  gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.qy.get(), op.np, one, sx, ld);
+}
+
+template void apply_hs<double>(Context&, KOperatorSet&, const double2*, long long, int, double2*, double2*, int);
+template void apply_hs<float>(Context&, KOperatorSet&, const float2*, long long, int, float2*, float2*, int);
+
+// Projector matrix of the prepared k point (used by the dense path and forces).
+const double2* projector_matrix64(KOperatorSet& ks) { return pick<double>(ks).B.get(); }
+
+}  // namespace hb

@@ -1,0 +1,632 @@
+// Context set-up on the device: the fixed-density effective potential and
+// the MIMIC_US QDEP correction D_ij^I with its position derivative.
+//
+// * Veff restates the ACC path's builder src/half_cuda_potential.cuf:270-350
+//   (Hartree + ionic local part in reciprocal space, PZ81 LDA or PBE with
+//   spectral gradients and finite-difference functional derivatives).
+// * D_ij^I and dD_ij^I/dR restate src/half_uspp.F90:112-241 (the CPU variant,
+//   which also provides dD/dR and symmetrises both); the GPU D-only variant
+//   src/half_cuda_uspp.cuf:124-195 is the same algorithm without symmetrising.
+// All full-box transforms use the library's own shared-memory FFT engine.
+#include <cmath>
+
+#include "context.h"
+
+namespace hb {
+
+// ------------------------------------------------------------------ runtime
+
+Runtime::Runtime() {
+  HALF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cublas_check(cublasCreate(&blas), "create");
+  cublas_check(cublasSetStream(blas, stream), "set stream");
+  cusolver_check(cusolverDnCreate(&solver), "create");
+  cusolver_check(cusolverDnSetStream(solver, stream), "set stream");
+  int v = 0;
+  cublasGetVersion(blas, &v);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  // FP32 emulation on BF16 tensor cores: cuBLAS >= 12.9 on compute capability 10.x
+  bf16x9 = (v >= 120900) && prop.major == 10;
+}
+
+Runtime::~Runtime() {
+  if (solver) cusolverDnDestroy(solver);
+  if (blas) cublasDestroy(blas);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// ------------------------------------------------------------------ 3-D FFT
+
+namespace {
+
+constexpr int kTile = 16;   // pencils per block for strided axes
+
+// FFT along the contiguous axis (i3): each block transforms `rows` pencils.
+template <typename C, typename R>
+__global__ void fft_rows_kernel(C* data, long long npencils, AxisPlan ap, int sign) {
+  extern __shared__ unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n = ap.plan.n;
+  C* buf = tw + kMaxFFT;
+  fill_twiddles(tw, n);
+  const long long p0 = (long long)blockIdx.x * kTile;
+  const int np = int(min((long long)kTile, npencils - p0));
+  for (int t = threadIdx.x; t < np * n; t += blockDim.x) buf[t] = data[p0 * n + t];
+  __syncthreads();
+  fft_pencils<false, C, R>(buf, np, n, 1, ap.plan, tw, sign);
+  for (int t = threadIdx.x; t < np * n; t += blockDim.x) {
+    int p = t / n, k = t - p * n;
+    data[(p0 + p) * n + k] = buf[p * n + ap.pos[k]];
+  }
+}
+
+// FFT along a strided axis: pencil (o, c) starts at o*outer_stride + c and
+// steps by axis_stride; a block takes kTile consecutive c (coalesced).
+template <typename C, typename R>
+__global__ void fft_strided_kernel(C* data, int ncols, long long axis_stride, long long outer_stride, AxisPlan ap,
+                                   int sign) {
+  extern __shared__ unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int n = ap.plan.n;
+  C* buf = tw + kMaxFFT;   // [k][tz]
+  fill_twiddles(tw, n);
+  const int c0 = blockIdx.x * kTile;
+  const int nc = min(kTile, ncols - c0);
+  const long long base = (long long)blockIdx.y * outer_stride + c0;
+  for (int t = threadIdx.x; t < n * kTile; t += blockDim.x) {
+    int k = t / kTile, c = t - k * kTile;
+    if (c < nc) buf[t] = data[base + k * axis_stride + c];
+    else buf[t] = cmake(R(0), R(0));
+  }
+  __syncthreads();
+  fft_pencils<false, C, R>(buf, kTile, 1, kTile, ap.plan, tw, sign);
+  for (int t = threadIdx.x; t < n * kTile; t += blockDim.x) {
+    int k = t / kTile, c = t - k * kTile;
+    if (c < nc) data[base + k * axis_stride + c] = buf[ap.pos[k] * kTile + c];
+  }
+}
+
+}  // namespace
+
+void fft3d_inplace(double2* data, const std::array<int, 3>& shape, int sign, cudaStream_t s) {
+  const int n1 = shape[0], n2 = shape[1], n3 = shape[2];
+  AxisPlan a1 = make_axis_plan(n1), a2 = make_axis_plan(n2), a3 = make_axis_plan(n3);
+  const long long rows = (long long)n1 * n2;
+  size_t sm3 = (kMaxFFT + size_t(kTile) * n3) * sizeof(double2);
+  fft_rows_kernel<double2, double><<<ceil_div(rows, kTile), 256, sm3, s>>>(data, rows, a3, sign);
+  HALF_LAUNCH("fft rows");
+  size_t sm2 = (kMaxFFT + size_t(kTile) * n2) * sizeof(double2);
+  fft_strided_kernel<double2, double><<<dim3(ceil_div(n3, kTile), n1), 256, sm2, s>>>(data, n3, n3, (long long)n2 * n3,
+                                                                                       a2, sign);
+  HALF_LAUNCH("fft axis 2");
+  size_t sm1 = (kMaxFFT + size_t(kTile) * n1) * sizeof(double2);
+  fft_strided_kernel<double2, double><<<dim3(ceil_div((long long)n2 * n3, kTile), 1), 256, sm1, s>>>(
+      data, n2 * n3, (long long)n2 * n3, 0, a1, sign);
+  HALF_LAUNCH("fft axis 1");
+}
+
+// ------------------------------------------------------------------ Veff
+
+namespace {
+
+struct Grid3 {
+  int n1, n2, n3;
+  double rec[9];
+};
+
+__device__ __forceinline__ void gvector(long long idx, const Grid3& g, double& qx, double& qy, double& qz) {
+  int i3 = int(idx % g.n3);
+  long long t = idx / g.n3;
+  int i2 = int(t % g.n2);
+  int i1 = int(t / g.n2);
+  int k1 = i1 <= (g.n1 - 1) / 2 ? i1 : i1 - g.n1;
+  int k2 = i2 <= (g.n2 - 1) / 2 ? i2 : i2 - g.n2;
+  int k3 = i3 <= (g.n3 - 1) / 2 ? i3 : i3 - g.n3;
+  qx = k1 * g.rec[0] + k2 * g.rec[3] + k3 * g.rec[6];
+  qy = k1 * g.rec[1] + k2 * g.rec[4] + k3 * g.rec[7];
+  qz = k1 * g.rec[2] + k2 * g.rec[5] + k3 * g.rec[8];
+}
+
+__global__ void reorder_f_to_c_kernel(const double* in, double* out, int n1, int n2, int n3) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)n1 * n2 * n3;
+  if (i >= n) return;
+  int i3 = int(i % n3);
+  long long t = i / n3;
+  int i2 = int(t % n2), i1 = int(t / n2);
+  out[i] = in[i1 + (long long)n1 * (i2 + (long long)n2 * i3)];
+}
+
+__global__ void real_to_complex_kernel(const double* in, double2* out, long long n, double scale) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_double2(in[i] * scale, 0.0);
+}
+
+__global__ void hartree_kernel(const double2* rho_g, double2* local_g, double2* core_g, Grid3 g, double volume) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)g.n1 * g.n2 * g.n3;
+  if (i >= n) return;
+  double qx, qy, qz;
+  gvector(i, g, qx, qy, qz);
+  double g2 = qx * qx + qy * qy + qz * qz;
+  double2 v = make_double2(0, 0);
+  if (g2 > 1.0e-12) v = cscale(rho_g[i], kEdeps / (g2 * volume));
+  local_g[i] = v;
+  core_g[i] = make_double2(0, 0);
+}
+
+__global__ void ionic_species_kernel(double2* local_g, double2* core_g, const double* y, const double* m2,
+                                     const double* cy, const double* cm2, int nrad, double gmax, double zval,
+                                     const double* pos, int natoms, Grid3 g, double volume, int has_core) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)g.n1 * g.n2 * g.n3;
+  if (i >= n) return;
+  double qx, qy, qz;
+  gvector(i, g, qx, qy, qz);
+  double g2 = qx * qx + qy * qy + qz * qz, gn = sqrt(g2);
+  double radial = spline_eval(y, m2, nrad, gmax, gn);
+  if (g2 > 1.0e-12) radial -= 4 * kPi * zval * kFelect / g2;
+  if (g2 <= 1.0e-12 || gn > gmax - gmax / nrad) radial = 0;
+  double core = 0;
+  if (has_core && gn <= gmax - 3 * gmax / nrad) core = spline_eval(cy, cm2, nrad, gmax, gn);
+  double sr = 0, si = 0;
+  for (int a = 0; a < natoms; ++a) {
+    double ph = qx * pos[3 * a] + qy * pos[3 * a + 1] + qz * pos[3 * a + 2];
+    double s, c;
+    sincos(ph, &s, &c);
+    sr += c;
+    si -= s;
+  }
+  double2 l = local_g[i], cg = core_g[i];
+  l.x += radial * sr / volume;
+  l.y += radial * si / volume;
+  cg.x += core * sr;
+  cg.y += core * si;
+  local_g[i] = l;
+  core_g[i] = cg;
+}
+
+__global__ void extract_real_kernel(const double2* in, double* out, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i].x;
+}
+
+// PZ81 LDA (src/half_cuda_potential.cuf:236-259)
+__global__ void lda_kernel(const double* charge, const double* core, const double* local_r, double* veff,
+                           long long n, double volume) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double density = (charge[i] + core[i]) / volume;
+  double rhoau = density * kAutoa * kAutoa * kAutoa;
+  if (rhoau <= 1.0e-30) { veff[i] = local_r[i]; return; }
+  double rs = cbrt(3.0 / (4 * kPi * rhoau));
+  double vx = -(4.0 / 3.0) * 0.4582 / rs, vc;
+  if (rs >= 1) {
+    double sr = sqrt(rs), denom = 1 + 1.0529 * sr + 0.3334 * rs;
+    double ec = -0.1423 / denom;
+    vc = ec * (1 + (7.0 / 6.0) * 1.0529 * sr + (4.0 / 3.0) * 0.3334 * rs) / denom;
+  } else {
+    double lnrs = log(rs);
+    vc = 0.0311 * lnrs + (-0.048 - 0.0311 / 3) + (2.0 / 3.0) * 0.002 * rs * lnrs + (-0.0232 - 0.002) * rs / 3;
+  }
+  veff[i] = local_r[i] + (vx + vc) * kHatoev;
+}
+
+__device__ double pw92_ec(double rs) {
+  const double a = .031091, a1 = .21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = .49294;
+  double sr = sqrt(rs);
+  double q = 2 * a * (b1 * sr + b2 * rs + b3 * rs * sr + b4 * rs * rs);
+  return -2 * a * (1 + a1 * rs) * log(1 + 1 / q);
+}
+
+// PBE energy density per volume (src/half_xc.F90:94-107)
+__device__ double pbe_energy_density(double density, double sigma) {
+  const double mu = 0.2195149727645171, kappa = 0.804, beta = 0.06672455060314922;
+  const double gamma = (1.0 - 0.69314718055994530942) / (kPi * kPi);
+  double n = fmax(density, 1.0e-30), s = fmax(sigma, 0.0);
+  double rs = cbrt(3 / (4 * kPi * n));
+  double kf = cbrt(3 * kPi * kPi * n);
+  double exlda = -3 * kf / (4 * kPi);
+  double s2 = s / (4 * kf * kf * n * n);
+  double fx = 1 + kappa - kappa / (1 + mu * s2 / kappa);
+  double ec = pw92_ec(rs);
+  double ks2 = 4 * kf / kPi;
+  double t2 = s / (4 * ks2 * n * n);
+  double aa = beta / gamma / (exp(-ec / gamma) - 1);
+  double at2 = aa * t2, ratio;
+  if (t2 == 0) ratio = 0;
+  else if (at2 < 1.0e100) ratio = t2 * (1 + at2) / (1 + at2 + at2 * at2);
+  else { double iv = 1 / at2; ratio = (1 / aa) * (1 + iv) / (1 + iv + iv * iv); }
+  double hh = gamma * log(1 + beta / gamma * ratio);
+  return n * (exlda * fx + ec + hh);
+}
+
+__global__ void pbe_density_kernel(const double* charge, const double* core, double* density, double2* work,
+                                   long long n, double volume) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double total = charge[i] + core[i];
+  density[i] = fmax(total / volume * kAutoa * kAutoa * kAutoa, 1.0e-20);
+  work[i] = make_double2(total / volume, 0.0);
+}
+
+__global__ void spectral_derivative_kernel(const double2* freq, double2* deriv, Grid3 g, int alpha) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)g.n1 * g.n2 * g.n3;
+  if (i >= n) return;
+  double qx, qy, qz;
+  gvector(i, g, qx, qy, qz);
+  double q = alpha == 0 ? qx : (alpha == 1 ? qy : qz);
+  double2 f = freq[i];
+  deriv[i] = make_double2(-q * f.y, q * f.x);
+}
+
+__global__ void accumulate_gradient_kernel(const double2* work, double* grad, double* sigma, long long n, int alpha) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a4 = kAutoa * kAutoa * kAutoa * kAutoa;
+  double gv = work[i].x / double(n) * a4;
+  grad[alpha * n + i] = gv;
+  sigma[i] = (alpha == 0 ? 0.0 : sigma[i]) + gv * gv;
+}
+
+__global__ void pbe_eval_kernel(const double* density, const double* sigma, double* fn, double* fs, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double d = density[i], s = sigma[i];
+  double dn = fmax(fabs(d) * 2.0e-5, 1.0e-12), nm = fmax(d - dn, 1.0e-30), np = d + dn;
+  fn[i] = (pbe_energy_density(np, s) - pbe_energy_density(nm, s)) / (np - nm);
+  double ds = fmax(fabs(s) * 2.0e-5, 1.0e-14), sm = fmax(s - ds, 0.0), sp = s + ds;
+  double f = (pbe_energy_density(d, sp) - pbe_energy_density(d, sm)) / (sp - sm);
+  fs[i] = d <= 1.0e-20 ? 0.0 : f;
+}
+
+__global__ void flux_kernel(const double* fs, const double* grad, double2* work, long long n, int alpha) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) work[i] = make_double2(2 * fs[i] * grad[alpha * n + i], 0.0);
+}
+
+__global__ void subtract_divergence_kernel(const double2* work, double* fn, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) fn[i] -= kAutoa * work[i].x / double(n);
+}
+
+__global__ void finish_pbe_kernel(const double* density, const double* local_r, const double* fn, double* veff,
+                                  long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = density[i] <= 1.0e-20 ? 0.0 : fn[i];
+  veff[i] = local_r[i] + v * kHatoev;
+}
+
+int blocks_for(long long n, int t = 256) { return ceil_div(n, t); }
+
+}  // namespace
+
+void build_veff_device(Context& ctx) {
+  cudaStream_t s = ctx.rt->stream;
+  const auto& sh = ctx.charge.shape;
+  const long long n = ctx.nr();
+  Grid3 g{sh[0], sh[1], sh[2], {}};
+  auto rec = ctx.crystal.reciprocal();
+  for (int i = 0; i < 9; ++i) g.rec[i] = rec[i];
+  const double vol = ctx.crystal.volume();
+  DeviceBuffer<double> raw(n), charge(n), local_r(n), core_r(n);
+  DeviceBuffer<double2> work(n), rho_g(n), local_g(n), core_g(n);
+  raw.upload(ctx.charge.values, s);
+  reorder_f_to_c_kernel<<<blocks_for(n), 256, 0, s>>>(raw.get(), charge.get(), sh[0], sh[1], sh[2]);
+  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), rho_g.get(), n, 1.0 / double(n));
+  fft3d_inplace(rho_g.get(), sh, -1, s);
+  hartree_kernel<<<blocks_for(n), 256, 0, s>>>(rho_g.get(), local_g.get(), core_g.get(), g, vol);
+  HALF_LAUNCH("hartree");
+  int ion0 = 0;
+  std::vector<DeviceBuffer<double>> keep;
+  for (size_t it = 0; it < ctx.pots.size(); ++it) {
+    const Potcar& p = ctx.pots[it];
+    int nat = ctx.crystal.counts[it];
+    auto m2 = spline_second(p.psp_local, p.psp_gmax);
+    std::vector<double> cy(p.psp_local.size(), 0.0), cm2(p.psp_local.size(), 0.0);
+    if (p.has_core()) { cy = p.pspcor; cm2 = spline_second(p.pspcor, p.psp_gmax); }
+    std::vector<double> pos;
+    for (int a = 0; a < nat; ++a) {
+      auto r = ctx.crystal.cartesian(ion0 + a);
+      pos.insert(pos.end(), r.begin(), r.end());
+    }
+    keep.emplace_back(); keep.back().upload(p.psp_local, s);
+    const double* dy = keep.back().get();
+    keep.emplace_back(); keep.back().upload(m2, s);
+    const double* dm2 = keep.back().get();
+    keep.emplace_back(); keep.back().upload(cy, s);
+    const double* dcy = keep.back().get();
+    keep.emplace_back(); keep.back().upload(cm2, s);
+    const double* dcm2 = keep.back().get();
+    keep.emplace_back(); keep.back().upload(pos, s);
+    const double* dpos = keep.back().get();
+    ionic_species_kernel<<<blocks_for(n), 256, 0, s>>>(local_g.get(), core_g.get(), dy, dm2, dcy, dcm2,
+                                                        int(p.psp_local.size()), p.psp_gmax, p.zval, dpos, nat, g, vol,
+                                                        p.has_core() ? 1 : 0);
+    HALF_LAUNCH("ionic species");
+    ion0 += nat;
+  }
+  fft3d_inplace(local_g.get(), sh, +1, s);
+  extract_real_kernel<<<blocks_for(n), 256, 0, s>>>(local_g.get(), local_r.get(), n);
+  fft3d_inplace(core_g.get(), sh, +1, s);
+  extract_real_kernel<<<blocks_for(n), 256, 0, s>>>(core_g.get(), core_r.get(), n);
+  ctx.veff.resize(n);
+  if (!ctx.use_pbe) {
+    lda_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), core_r.get(), local_r.get(), ctx.veff.get(), n, vol);
+    HALF_LAUNCH("lda");
+  } else {
+    DeviceBuffer<double> density(n), sigma(n), grad(3 * n), fn(n), fs(n);
+    DeviceBuffer<double2> freq(n), deriv(n);
+    pbe_density_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), core_r.get(), density.get(), freq.get(), n, vol);
+    fft3d_inplace(freq.get(), sh, -1, s);
+    for (int a = 0; a < 3; ++a) {
+      spectral_derivative_kernel<<<blocks_for(n), 256, 0, s>>>(freq.get(), deriv.get(), g, a);
+      fft3d_inplace(deriv.get(), sh, +1, s);
+      accumulate_gradient_kernel<<<blocks_for(n), 256, 0, s>>>(deriv.get(), grad.get(), sigma.get(), n, a);
+    }
+    pbe_eval_kernel<<<blocks_for(n), 256, 0, s>>>(density.get(), sigma.get(), fn.get(), fs.get(), n);
+    for (int a = 0; a < 3; ++a) {
+      flux_kernel<<<blocks_for(n), 256, 0, s>>>(fs.get(), grad.get(), work.get(), n, a);
+      fft3d_inplace(work.get(), sh, -1, s);
+      spectral_derivative_kernel<<<blocks_for(n), 256, 0, s>>>(work.get(), deriv.get(), g, a);
+      fft3d_inplace(deriv.get(), sh, +1, s);
+      subtract_divergence_kernel<<<blocks_for(n), 256, 0, s>>>(deriv.get(), fn.get(), n);
+    }
+    finish_pbe_kernel<<<blocks_for(n), 256, 0, s>>>(density.get(), local_r.get(), fn.get(), ctx.veff.get(), n);
+    HALF_LAUNCH("pbe");
+    HALF_CUDA(cudaStreamSynchronize(s));
+  }
+  HALF_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------------------------ QDEP
+
+namespace {
+
+__global__ void prefilter_kernel(double2* freq, int n1, int n2, int n3) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long n = (long long)n1 * n2 * n3;
+  if (i >= n) return;
+  int i3 = int(i % n3);
+  long long t = i / n3;
+  int i2 = int(t % n2), i1 = int(t / n2);
+  double b1 = (2.0 + cospi(2.0 * i1 / n1)) / 3.0;
+  double b2 = (2.0 + cospi(2.0 * i2 / n2)) / 3.0;
+  double b3 = (2.0 + cospi(2.0 * i3 / n3)) / 3.0;
+  freq[i] = cscale(freq[i], 1.0 / (b1 * b2 * b3));
+}
+
+__global__ void coeff_real_kernel(const double2* in, double* out, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i].x / double(n);
+}
+
+__device__ __forceinline__ void cubic_w(double t, double* w) {
+  double u = 1 - t;
+  w[0] = u * u * u / 6;
+  w[1] = (3 * t * t * t - 6 * t * t + 4) / 6;
+  w[2] = (-3 * t * t * t + 3 * t * t + 3 * t + 1) / 6;
+  w[3] = t * t * t / 6;
+}
+__device__ __forceinline__ void cubic_dw(double t, double* w) {
+  w[0] = -0.5 * (1 - t) * (1 - t);
+  w[1] = 1.5 * t * t - 2.0 * t;
+  w[2] = -1.5 * t * t + t + 0.5;
+  w[3] = 0.5 * t * t;
+}
+
+struct SampleGeom {
+  int n1, n2, n3;
+  double inv[9];   // inverse lattice, row-major
+};
+
+// One sample per (atom, radial point, direction): value and Cartesian
+// gradient of the cubic B-spline interpolant (src/half_uspp.F90:243-277).
+__global__ void sample_kernel(const double* coeff, const double* pos, const double* rgrid, const double* dirs,
+                              int natoms, int nrad, int nang, SampleGeom g, int gradient, double* out) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long total = (long long)natoms * nrad * nang;
+  if (idx >= total) return;
+  int ip = int(idx % nang);
+  long long t = idx / nang;
+  int ir = int(t % nrad), a = int(t / nrad);
+  double cart[3], frac[3];
+  for (int j = 0; j < 3; ++j) cart[j] = pos[3 * a + j] + rgrid[ir] * dirs[3 * ip + j];
+  for (int j = 0; j < 3; ++j) {
+    double f = cart[0] * g.inv[0 * 3 + j] + cart[1] * g.inv[1 * 3 + j] + cart[2] * g.inv[2 * 3 + j];
+    frac[j] = f - floor(f);
+  }
+  int nn[3] = {g.n1, g.n2, g.n3};
+  int ix[3];
+  double w[3][4], dw[3][4];
+  for (int j = 0; j < 3; ++j) {
+    double c = frac[j] * nn[j];
+    ix[j] = int(floor(c));
+    cubic_w(c - ix[j], w[j]);
+    cubic_dw(c - ix[j], dw[j]);
+  }
+  double v = 0, df0 = 0, df1 = 0, df2 = 0;
+  for (int p = 0; p < 4; ++p) {
+    int ia = ((ix[0] + p - 1) % g.n1 + g.n1) % g.n1;
+    for (int q = 0; q < 4; ++q) {
+      int ib = ((ix[1] + q - 1) % g.n2 + g.n2) % g.n2;
+      const double* row = coeff + ((long long)ia * g.n2 + ib) * g.n3;
+      for (int r = 0; r < 4; ++r) {
+        int ic = ((ix[2] + r - 1) % g.n3 + g.n3) % g.n3;
+        double c = row[ic];
+        v += w[0][p] * w[1][q] * w[2][r] * c;
+        if (gradient) {
+          df0 += dw[0][p] * w[1][q] * w[2][r] * c * g.n1;
+          df1 += w[0][p] * dw[1][q] * w[2][r] * c * g.n2;
+          df2 += w[0][p] * w[1][q] * dw[2][r] * c * g.n3;
+        }
+      }
+    }
+  }
+  out[idx] = v;
+  if (gradient) {
+    for (int al = 0; al < 3; ++al)
+      out[(al + 1) * total + idx] = df0 * g.inv[al * 3 + 0] + df1 * g.inv[al * 3 + 1] + df2 * g.inv[al * 3 + 2];
+  }
+}
+
+// radial[c][a][k] = sum_ir wr2g[k][ir] sum_ip samples[c][a][ir][ip] yweight[ip][k]
+__global__ void project_radial_kernel(const double* samples, const double* yweight, const double* wr2g, int natoms,
+                                      int nrad, int nang, int naug, int ncomp, double* radial) {
+  int k = blockIdx.x, a = blockIdx.y, c = blockIdx.z;
+  if (k >= naug || a >= natoms || c >= ncomp) return;
+  long long total = (long long)natoms * nrad * nang;
+  double acc = 0;
+  for (int ir = threadIdx.x; ir < nrad; ir += blockDim.x) {
+    const double* s = samples + c * total + ((long long)a * nrad + ir) * nang;
+    double v = 0;
+    for (int ip = 0; ip < nang; ++ip) v += s[ip] * yweight[ip * naug + k];
+    acc += wr2g[(long long)k * nrad + ir] * v;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) radial[((long long)c * natoms + a) * naug + k] = red[0];
+}
+
+// D = DION + multipole . radial_v (symmetrised); dD_alpha = multipole . radial_grad_alpha
+__global__ void finish_dij_kernel(const double* dion, const double* mp, const double* radial, int natoms, int nlm,
+                                  int naug, int ncomp, double* dij, double* ddij) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  long long total = (long long)natoms * nlm * nlm;
+  if (idx >= total) return;
+  int b = int(idx % nlm);
+  long long t = idx / nlm;
+  int a = int(t % nlm), at = int(t / nlm);
+  for (int c = 0; c < ncomp; ++c) {
+    const double* rv = radial + ((long long)c * natoms + at) * naug;
+    double vab = 0, vba = 0;
+    for (int k = 0; k < naug; ++k) {
+      vab += mp[((long long)a * nlm + b) * naug + k] * rv[k];
+      vba += mp[((long long)b * nlm + a) * naug + k] * rv[k];
+    }
+    if (c == 0) {
+      vab += dion[a * nlm + b];
+      vba += dion[b * nlm + a];
+      dij[idx] = 0.5 * (vab + vba);
+    } else {
+      ddij[(((long long)at * 3 + (c - 1)) * nlm + a) * nlm + b] = 0.5 * (vab + vba);
+    }
+  }
+}
+
+}  // namespace
+
+void build_dij_device(Context& ctx, bool gradient) {
+  cudaStream_t s = ctx.rt->stream;
+  const auto& sh = ctx.charge.shape;
+  const long long n = ctx.nr();
+  DeviceBuffer<double2> freq(n);
+  DeviceBuffer<double> coeff(n);
+  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(ctx.veff.get(), freq.get(), n, 1.0);
+  fft3d_inplace(freq.get(), sh, -1, s);
+  prefilter_kernel<<<blocks_for(n), 256, 0, s>>>(freq.get(), sh[0], sh[1], sh[2]);
+  fft3d_inplace(freq.get(), sh, +1, s);
+  coeff_real_kernel<<<blocks_for(n), 256, 0, s>>>(freq.get(), coeff.get(), n);
+  HALF_LAUNCH("qdep prefilter");
+  SampleGeom geom{sh[0], sh[1], sh[2], {}};
+  auto inv = ctx.crystal.inverse_lattice();
+  for (int i = 0; i < 9; ++i) geom.inv[i] = inv[i];
+  const int ncomp = gradient ? 4 : 1;
+  for (auto& sp : ctx.species) {
+    const QdepTables& t = sp.tables;
+    const int nang = int(t.dirs.size() / 3);
+    std::vector<double> pos;
+    for (int a = 0; a < sp.natoms; ++a) {
+      auto r = ctx.crystal.cartesian(sp.first_ion + a);
+      pos.insert(pos.end(), r.begin(), r.end());
+    }
+    DeviceBuffer<double> dpos, drg, ddirs, dyw, dwr, dmp, ddion, samples, radial;
+    dpos.upload(pos, s);
+    drg.upload(t.rgrid, s);
+    ddirs.upload(t.dirs, s);
+    dyw.upload(t.yweight, s);
+    dwr.upload(t.wr2g, s);
+    dmp.upload(t.multipole, s);
+    ddion.upload(t.dion_lm, s);
+    long long total = (long long)sp.natoms * t.nrad * nang;
+    samples.resize(size_t(total) * ncomp);
+    radial.resize(size_t(ncomp) * sp.natoms * t.naug);
+    sample_kernel<<<blocks_for(total), 256, 0, s>>>(coeff.get(), dpos.get(), drg.get(), ddirs.get(), sp.natoms, t.nrad,
+                                                     nang, geom, gradient ? 1 : 0, samples.get());
+    HALF_LAUNCH("qdep sample");
+    project_radial_kernel<<<dim3(t.naug, sp.natoms, ncomp), 256, 0, s>>>(samples.get(), dyw.get(), dwr.get(), sp.natoms,
+                                                                          t.nrad, nang, t.naug, ncomp, radial.get());
+    HALF_LAUNCH("qdep radial");
+    sp.dij.resize(size_t(sp.natoms) * sp.nlm * sp.nlm);
+    sp.ddij.resize(size_t(sp.natoms) * 3 * sp.nlm * sp.nlm);
+    if (!gradient) sp.ddij.zero(s);
+    long long npair = (long long)sp.natoms * sp.nlm * sp.nlm;
+    finish_dij_kernel<<<blocks_for(npair), 256, 0, s>>>(ddion.get(), dmp.get(), radial.get(), sp.natoms, sp.nlm, t.naug,
+                                                         ncomp, sp.dij.get(), sp.ddij.get());
+    HALF_LAUNCH("qdep finish");
+    HALF_CUDA(cudaStreamSynchronize(s));
+    sp.dij_host = sp.dij.download(s);
+  }
+}
+
+// ------------------------------------------------------------------ context
+
+void Context::initialize() {
+  if (!rt) rt = std::make_unique<Runtime>();
+  for (int j = 0; j < 3; ++j) make_fft_plan(charge.shape[j]);   // validates the box
+  species.clear();
+  species.resize(pots.size());
+  int ion0 = 0;
+  for (size_t it = 0; it < pots.size(); ++it) {
+    SpeciesDevice& sp = species[it];
+    const Potcar& p = pots[it];
+    sp.natoms = crystal.counts[it];
+    sp.nlm = p.nlm();
+    sp.first_ion = ion0;
+    sp.lps = p.lps;
+    sp.nchan = p.channels();
+    sp.pspnl_gmax = p.pspnl_gmax;
+    sp.tables = build_qdep_tables(p);
+    sp.qij_host = sp.tables.qij_lm;
+    sp.qij.upload(sp.qij_host, rt->stream);
+    sp.radial_y.clear();
+    sp.radial_m2.clear();
+    for (int c = 0; c < sp.nchan; ++c) {
+      std::vector<double> y(p.pspnl.begin() + c * 100, p.pspnl.begin() + (c + 1) * 100);
+      auto m2 = spline_second(y, p.pspnl_gmax);
+      sp.radial_y.insert(sp.radial_y.end(), y.begin(), y.end());
+      sp.radial_m2.insert(sp.radial_m2.end(), m2.begin(), m2.end());
+    }
+    ion0 += sp.natoms;
+  }
+  build_veff_device(*this);
+  rebuild_dij();
+}
+
+void Context::rebuild_dij() {
+  if (use_uspp) {
+    build_dij_device(*this, true);
+    return;
+  }
+  for (auto& sp : species) {   // DION only, the same for every atom (src/half_cuda_assembly.cuf:443-446)
+    sp.dij_host.clear();
+    for (int a = 0; a < sp.natoms; ++a)
+      sp.dij_host.insert(sp.dij_host.end(), sp.tables.dion_lm.begin(), sp.tables.dion_lm.end());
+    sp.dij.upload(sp.dij_host, rt->stream);
+    sp.ddij.resize(size_t(sp.natoms) * 3 * sp.nlm * sp.nlm);
+    sp.ddij.zero(rt->stream);
+  }
+  HALF_CUDA(cudaStreamSynchronize(rt->stream));
+}
+
+}  // namespace hb

@@ -1,0 +1,94 @@
+/* Additive extensions to libhalf ABI v1 (B200 build).
+ *
+ * None of these symbols exists in the reference; they are the "additive
+ * extensions" its docs/API.md:111-112 anticipates.  Each comment names the
+ * reference routine whose behaviour the call exposes.  All calls follow the
+ * ABI v1 conventions of half.h (status return, caller-owned buffers, error
+ * buffer cleared on entry, complex128 column-major).
+ */
+#ifndef DEEPAW_HALF_B200_H
+#define DEEPAW_HALF_B200_H
+
+#include "half.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum half_precision {
+  HALF_PRECISION_FP64 = 0,   /* every operator application and GEMM in FP64 */
+  HALF_PRECISION_MIXED = 1   /* FP32 operator / tensor-core GEMMs, FP64 refinement */
+};
+
+/* ACC controls.  The reference's solve_block_harris_cuda_full takes
+ * tolerance / max_iterations / block_size (src/half_cuda_iterative_solver.cuf:
+ * 113-119; CLI --acc-tol, --acc-max-iter, --acc-block-size) but ABI v1 never
+ * passes them, so the defaults 1e-4 eV / 40 / 16 apply (src/half_library.F90:
+ * 343-367).  This setter keeps those defaults until it is called.
+ * tolerance_eV > 0, max_iterations >= 1, block_size >= 1, precision one of
+ * half_precision; otherwise HALF_ERROR_INVALID_ARGUMENT. */
+int half_set_acc_controls(half_handle handle, double tolerance_eV,
+                          int max_iterations, int block_size, int precision,
+                          char *error, int error_capacity);
+
+/* Diagnostics of the last solve on this context (the reference reports the
+ * same figures through its CLI JSON: iterative_solver_iterations, final
+ * residual, phase seconds; app/half_cli.F90:306-349). */
+typedef struct half_solve_info_v1 {
+  uint32_t struct_size;        /* set to sizeof(half_solve_info_v1) */
+  int32_t iterations;          /* ACC iterations (all phases) */
+  int32_t fp64_iterations;     /* of which in the FP64 refinement phase */
+  int32_t converged;           /* 1 when max residual <= tolerance */
+  int64_t npw;
+  int64_t operator_applications;  /* band-columns pushed through H/S */
+  double max_residual_eV;
+  double setup_ms;             /* basis, projectors, operator tables */
+  double solve_ms;             /* iterations through eigenpairs */
+  double operator_ms;          /* time inside H/S applications */
+  uint64_t reserved[6];
+} half_solve_info_v1;
+int half_get_last_solve_info(half_handle handle, half_solve_info_v1 *info,
+                             char *error, int error_capacity);
+
+/* Solve several k points in one call (eigenvalues only, row-major
+ * [ik][band]).  Same per-k algorithm as half_solve_kpoint; the k points are
+ * independent units (the reference distributes them cyclically over MPI
+ * ranks, src/half_parallel.F90:62-65). */
+int half_solve_kpoints(half_handle handle, int nk, const double *kpoints,
+                       int nbands, double *eigenvalues_eV,
+                       char *error, int error_capacity);
+
+/* Move the atoms at fixed Veff (positions fractional, atom-major, in the
+ * context's type-major order).  Rebuilds the MIMIC_US D_ij and dD_ij/dR
+ * (src/half_uspp.F90:137-241) and, at the next solve, the projector phases
+ * (src/half_paw.F90:52-65).  This is the perturbation the finite-difference
+ * force oracle applies. */
+int half_set_positions(half_handle handle, const double *positions_fractional,
+                       char *error, int error_capacity);
+
+/* Non-local PAW band-energy force for given eigenpairs at one k point
+ * (src/half_forces.F90:9-73), accumulated into forces[nions*3] (atom-major,
+ * eV/A).  vectors: npw x nbands, leading dimension ld >= npw; bands with zero
+ * occupation are skipped exactly as in the reference. */
+int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands,
+                         int64_t ld, const HALF_C128 *vectors,
+                         const double *eigenvalues_eV,
+                         const double *occupations, double kweight,
+                         double *forces, char *error, int error_capacity);
+
+/* The band-energy force workload end to end: solve nk k points with the
+ * context's solver, compute occupations for nelect electrons with width
+ * sigma (ismear -1 Fermi-Dirac, 0 Gaussian; src/half_energy.F90:41-120), then
+ * the non-local force on the GPU.  Optional outputs may be NULL:
+ * eigenvalues [nk][nbands], occupations [nk][nbands], energies[3] =
+ * {band energy, entropy term, chemical potential}. */
+int half_band_forces(half_handle handle, int nk, const double *kpoints,
+                     const double *kweights, int nbands, double nelect,
+                     double sigma, int ismear, double *forces,
+                     double *eigenvalues_eV, double *occupations,
+                     double *energies, char *error, int error_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
