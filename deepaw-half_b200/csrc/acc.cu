@@ -245,6 +245,7 @@ void project_upper(Runtime& rt, int n, int m, const cplx_t<R>* x, const cplx_t<R
   if constexpr (sizeof(R) == 4) {
     long long tot = 4LL * m * m;
     convert_kernel<float2, double2><<<ceil_div(tot, 256), 256, 0, rt.stream>>>(tmp2m, out, tot);
+    ++rt.prof.launches;
   }
 }
 
@@ -278,6 +279,7 @@ struct AccRun {
     } else {
       convert_block_kernel<double2, float2><<<ceil_div((long long)rows * cols, 256), 256, 0, rt.stream>>>(in, ldi, out, ldo,
                                                                                                        rows, cols);
+      ++rt.prof.launches;
     }
   }
 
@@ -292,8 +294,10 @@ struct AccRun {
     } else {
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.hx(), n, zero, tmp2m.get(), m);
       convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(tmp2m.get(), hs, (long long)m * m);
+      ++rt.prof.launches;
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.sx(), n, zero, tmp2m.get(), m);
       convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(tmp2m.get(), ssb, (long long)m * m);
+      ++rt.prof.launches;
     }
     ss.hegvd(hs, ssb, m, sc.w.get());
     to_r(hs, m, blk.Y.get(), m, m, m);
@@ -307,6 +311,7 @@ struct AccRun {
   // residual norms of the current Ritz pairs; returns max norm (host sync)
   double residuals(std::vector<double>& norms, int* infos) {
     residual_norm_kernel<C><<<m, 256, 0, rt.stream>>>(blk.hx(), blk.sx(), n, n, sc.w.get(), sc.norms.get());
+    ++rt.prof.launches;
     HALF_LAUNCH("residual norms");
     norms.resize(m);
     HALF_CUDA(cudaMemcpyAsync(norms.data(), sc.norms.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
@@ -326,6 +331,7 @@ struct AccRun {
     precondition_kernel<C><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(blk.hx(), blk.sx(), n, n, m, sc.w.get(),
                                                                        sc.norms.get(), seed_threshold, sc.kinetic.get(),
                                                                        blk.P.get());
+    ++rt.prof.launches;
     HALF_LAUNCH("precondition");
     apply(blk.P.get(), blk.HP.get(), blk.SP.get(), m);
     // S-orthogonalise against X
@@ -341,9 +347,11 @@ struct AccRun {
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.P.get(), n, blk.SP.get(), n, zero, blk.small.get(), m);
       convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(blk.small.get(), metric,
                                                                                                (long long)m * m);
+      ++rt.prof.launches;
     }
     ss.heevd(metric, m, sc.mu.get());
     scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14);
+    ++rt.prof.launches;
     to_r(metric, m, blk.small.get(), m, m, m);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.P.get(), n, blk.small.get(), m, zero, blk.PU.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HP.get(), n, blk.small.get(), m, zero, blk.HPU.get(), n);
@@ -417,6 +425,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     DeviceBuffer<float2> tmp32(size_t(4) * m * m);
     AccRun<float> run32{ctx, ks, rt, b32, sc, ss, tmp32, n, m, cfg.block};
     init_states_kernel<float2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b32.x(), n, n, m, sc.idx.get());
+    ++rt.prof.launches;
     run32.apply(b32.x(), b32.hx(), b32.sx(), m);
     run32.rayleigh_ritz_x();
     // Switch to FP64 once the residual is in the FP32 regime or stops improving.
@@ -434,6 +443,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     op_cols += run32.op_cols;
     // promote X, recreate H X and S X in FP64, Rayleigh-Ritz
     convert_kernel<float2, double2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b32.x(), b64.x(), (long long)n * m);
+    ++rt.prof.launches;
     run64.apply(b64.x(), b64.hx(), b64.sx(), m);
     run64.rayleigh_ritz_x();
     for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
@@ -445,6 +455,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     iter += fp64_iter;
   } else {
     init_states_kernel<double2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b64.x(), n, n, m, sc.idx.get());
+    ++rt.prof.launches;
     run64.apply(b64.x(), b64.hx(), b64.sx(), m);
     run64.rayleigh_ritz_x();
     for (iter = 1; iter <= cfg.max_iter; ++iter) {

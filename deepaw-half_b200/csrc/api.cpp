@@ -136,11 +136,35 @@ int create_context(const std::string& charge, const std::string& potential, doub
   });
 }
 
+// Event accounting around one device call (solve, H/S application, force).
+void begin_call(Context& ctx) {
+  Profile& pf = ctx.rt->prof;
+  pf.reset();
+  HALF_CUDA(cudaEventRecord(pf.a, ctx.rt->stream));
+}
+
+void end_call(Context& ctx) {
+  Profile& pf = ctx.rt->prof;
+  HALF_CUDA(cudaEventRecord(pf.b, ctx.rt->stream));
+  HALF_CUDA(cudaEventSynchronize(pf.b));
+  float ms = 0;
+  HALF_CUDA(cudaEventElapsedTime(&ms, pf.a, pf.b));
+  ctx.last.device_ms = ms;
+  ctx.last.local_ms = pf.local_ms;
+  ctx.last.local_bytes = pf.local_bytes;
+  ctx.last.local_columns = pf.local_columns;
+  ctx.last.launches = pf.launches;
+  ctx.last.sweep_ms = pf.sweep_ms;
+  ctx.last.sweep_columns = pf.sweep_columns;
+  ctx.last.adjoint_ms = pf.adjoint_ms;
+}
+
 // Solve one k point with the context's solver; out holds device vectors.
 void solve_one(Context& ctx, const double k[3], int nbands, bool want_vectors, SolveOutput& out,
                std::unique_ptr<KOperatorSet>* keep = nullptr) {
   auto t0 = std::chrono::steady_clock::now();
   if (!finite3(k)) fail(kInvalidArgument, "k point must be finite");
+  begin_call(ctx);
   bool mixed = ctx.solver == HALF_SOLVER_ACC && ctx.acc.precision == kMixed;
   auto ks = prepare_operator(ctx, k, true, mixed);
   double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -153,6 +177,7 @@ void solve_one(Context& ctx, const double k[3], int nbands, bool want_vectors, S
   }
   ctx.last.setup_ms = setup_ms;
   ctx.last.npw = ks->basis.npw();
+  end_call(ctx);
   if (keep) *keep = std::move(ks);
 }
 
@@ -374,7 +399,10 @@ int half_apply_hs(half_handle handle, const double kpoint[3], int nstates, int64
     DeviceBuffer<double2> x((size_t)n * nstates), hx((size_t)n * nstates), sx((size_t)n * nstates);
     HALF_CUDA(cudaMemcpy2DAsync(x.get(), n * sizeof(double2), psi, ld * sizeof(double2), n * sizeof(double2), nstates,
                                 cudaMemcpyHostToDevice, st));
+    ctx->last = SolveInfo();
+    begin_call(*ctx);
     apply_hs<double>(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
+    end_call(*ctx);
     HALF_CUDA(cudaMemcpy2DAsync(hpsi, ld * sizeof(double2), hx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
                                 cudaMemcpyDeviceToHost, st));
     HALF_CUDA(cudaMemcpy2DAsync(spsi, ld * sizeof(double2), sx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
@@ -512,6 +540,14 @@ int half_get_last_solve_info(half_handle handle, half_solve_info_v1* info, char*
   info->setup_ms = s.setup_ms;
   info->solve_ms = s.solve_ms;
   info->operator_ms = s.operator_ms;
+  info->device_ms = s.device_ms;
+  info->local_ms = s.local_ms;
+  info->local_bytes = s.local_bytes;
+  info->local_columns = s.local_columns;
+  info->kernel_launches = s.launches;
+  info->sweep_ms = s.sweep_ms;
+  info->sweep_columns = s.sweep_columns;
+  info->adjoint_ms = s.adjoint_ms;
   std::memset(info->reserved, 0, sizeof(info->reserved));
   return HALF_SUCCESS;
 }
@@ -540,6 +576,13 @@ int half_solve_kpoints(half_handle handle, int nk, const double* kpoints, int nb
       total.solve_ms += ctx->last.solve_ms;
       total.operator_ms += ctx->last.operator_ms;
       total.npw += ctx->last.npw;
+      total.device_ms += ctx->last.device_ms;
+      total.local_ms += ctx->last.local_ms;
+      total.local_bytes += ctx->last.local_bytes;
+      total.local_columns += ctx->last.local_columns;
+      total.launches += ctx->last.launches;
+      total.sweep_ms += ctx->last.sweep_ms;
+      total.sweep_columns += ctx->last.sweep_columns;
     }
     ctx->last = total;
     return HALF_SUCCESS;
@@ -580,7 +623,10 @@ int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands,
     DeviceBuffer<double2> dv((size_t)n * nbands);
     HALF_CUDA(cudaMemcpy2DAsync(dv.get(), n * sizeof(double2), vectors, ld * sizeof(double2), n * sizeof(double2),
                                 nbands, cudaMemcpyHostToDevice, st));
+    ctx->last = SolveInfo();
+    begin_call(*ctx);
     nonlocal_forces_device(*ctx, *ks, dv.get(), n, nbands, eigenvalues, occupations, kweight, forces);
+    end_call(*ctx);
     return HALF_SUCCESS;
   });
 }

@@ -27,6 +27,25 @@ struct SolveInfo {
   int iterations = 0, fp64_iterations = 0, converged = 0;
   long long npw = 0, operator_columns = 0;
   double max_residual = 0, setup_ms = 0, solve_ms = 0, operator_ms = 0;
+  double device_ms = 0;          // CUDA-event span on the context stream, prepare -> eigenpairs
+  double local_ms = 0;           // CUDA-event time inside the local-operator kernels
+  double local_bytes = 0;        // their algorithmic bytes (per-band FFT-path figure)
+  long long local_columns = 0;   // band columns through the local operator
+  long long launches = 0;        // library kernels launched
+  double sweep_ms = 0;           // CUDA-event time of whole H/S applications
+  long long sweep_columns = 0;
+  double adjoint_ms = 0;         // CUDA-event time of the force adjoint
+};
+
+// Event-based accounting of the library's own kernels.
+struct Profile {
+  cudaEvent_t a = nullptr, b = nullptr, la = nullptr, lb = nullptr, sa = nullptr, sb = nullptr;
+  double local_ms = 0, local_bytes = 0, sweep_ms = 0, adjoint_ms = 0;
+  long long local_columns = 0, launches = 0, sweep_columns = 0;
+  void reset() {
+    local_ms = local_bytes = sweep_ms = adjoint_ms = 0;
+    local_columns = launches = sweep_columns = 0;
+  }
 };
 
 // Per-stream library handles.
@@ -35,6 +54,7 @@ struct Runtime {
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
   bool bf16x9 = false;   // cuBLAS offers FP32 emulation on BF16 tensor cores
+  Profile prof;
   Runtime();
   ~Runtime();
   Runtime(const Runtime&) = delete;

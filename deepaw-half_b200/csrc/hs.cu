@@ -425,6 +425,10 @@ KOperator<float>& pick<float>(KOperatorSet& ks) {
 }
 
 template <typename R>
+void apply_nonlocal(Runtime& rt, KOperator<R>& op, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx,
+                    cplx_t<R>* sx);
+
+template <typename R>
 void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx, cplx_t<R>* sx,
               int chunk) {
   using C = cplx_t<R>;
@@ -439,6 +443,9 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
   }
   const size_t psm = plane_smem<R>(op.n2, op.n3), xsm = xline_smem<R>(op.n1, op.nplanes);
   const int tiles = (op.n3 + kXTile - 1) / kXTile;
+  Profile& pf = rt.prof;
+  HALF_CUDA(cudaEventRecord(pf.sa, s));
+  HALF_CUDA(cudaEventRecord(pf.la, s));
   for (int b0 = 0; b0 < nb; b0 += chunk) {
     int nbc = std::min(chunk, nb - b0);
     k1_sphere_to_planes<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
@@ -449,9 +456,39 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
     k3_planes_to_sphere<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
         op.work.get(), op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(),
         op.row_list.get(), op.ay, op.az, x, ld, b0, op.kinetic.get(), hx, sx);
+    pf.launches += 3;
   }
   HALF_LAUNCH("local operator");
-  if (op.np == 0) return;
+  HALF_CUDA(cudaEventRecord(pf.lb, s));
+  {
+    // FFT-path algorithmic bytes per band: read psi, write H psi and S psi, two
+    // transforms x two passes x (read + write) of the box; Veff once per call.
+    const double sz = sizeof(C), rz = sizeof(R), nr = double(op.n1) * op.n2 * op.n3;
+    pf.local_bytes += nb * (3.0 * sz * op.npw + 8.0 * sz * nr) + rz * nr;
+    pf.local_columns += nb;
+    HALF_CUDA(cudaEventSynchronize(pf.lb));
+    float ms = 0;
+    HALF_CUDA(cudaEventElapsedTime(&ms, pf.la, pf.lb));
+    pf.local_ms += ms;
+  }
+  if (op.np > 0) {
+    pf.launches += 1;
+    apply_nonlocal<R>(rt, op, x, ld, nb, hx, sx);
+  }
+  HALF_CUDA(cudaEventRecord(pf.sb, s));
+  HALF_CUDA(cudaEventSynchronize(pf.sb));
+  float sms = 0;
+  HALF_CUDA(cudaEventElapsedTime(&sms, pf.sa, pf.sb));
+  pf.sweep_ms += sms;
+  pf.sweep_columns += nb;
+}
+
+// Projector part: H X += B blockdiag(D) B^H X, S X += B blockdiag(Q) B^H X
+template <typename R>
+void apply_nonlocal(Runtime& rt, KOperator<R>& op, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx,
+                    cplx_t<R>* sx) {
+  using C = cplx_t<R>;
+  cudaStream_t s = rt.stream;
   if (op.ws_cols < nb) {
     op.coeff.resize((size_t)op.np * nb);
     op.dy.resize((size_t)op.np * nb);

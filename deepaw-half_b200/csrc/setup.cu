@@ -28,11 +28,21 @@ Runtime::Runtime() {
   cudaGetDevice(&dev);
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, dev);
-  // FP32 emulation on BF16 tensor cores: cuBLAS >= 12.9 on compute capability 10.x
+  // FP32 emulation on BF16 tensor cores: cuBLAS >= 12.9 on compute capability 10.x.
+  // The math mode only affects FP32 routines, i.e. the mixed-precision GEMMs.
   bf16x9 = (v >= 120900) && prop.major == 10;
+  if (bf16x9 && cublasSetMathMode(blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) != CUBLAS_STATUS_SUCCESS) bf16x9 = false;
+  HALF_CUDA(cudaEventCreate(&prof.a));
+  HALF_CUDA(cudaEventCreate(&prof.b));
+  HALF_CUDA(cudaEventCreate(&prof.la));
+  HALF_CUDA(cudaEventCreate(&prof.lb));
+  HALF_CUDA(cudaEventCreate(&prof.sa));
+  HALF_CUDA(cudaEventCreate(&prof.sb));
 }
 
 Runtime::~Runtime() {
+  for (cudaEvent_t e : {prof.a, prof.b, prof.la, prof.lb, prof.sa, prof.sb})
+    if (e) cudaEventDestroy(e);
   if (solver) cusolverDnDestroy(solver);
   if (blas) cublasDestroy(blas);
   if (stream) cudaStreamDestroy(stream);

@@ -43,7 +43,10 @@ class SolveInfo(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("iterations", C.c_int32), ("fp64_iterations", C.c_int32),
                 ("converged", C.c_int32), ("npw", C.c_int64), ("operator_applications", C.c_int64),
                 ("max_residual_eV", C.c_double), ("setup_ms", C.c_double), ("solve_ms", C.c_double),
-                ("operator_ms", C.c_double), ("reserved", C.c_uint64 * 6)]
+                ("operator_ms", C.c_double), ("device_ms", C.c_double), ("local_ms", C.c_double),
+                ("local_bytes", C.c_double), ("local_columns", C.c_int64), ("kernel_launches", C.c_int64),
+                ("sweep_ms", C.c_double), ("sweep_columns", C.c_int64), ("adjoint_ms", C.c_double),
+                ("reserved", C.c_uint64 * 4)]
 
 
 class RequestGeometry(C.Structure):

@@ -31,9 +31,11 @@ int half_set_acc_controls(half_handle handle, double tolerance_eV,
                           int max_iterations, int block_size, int precision,
                           char *error, int error_capacity);
 
-/* Diagnostics of the last solve on this context (the reference reports the
- * same figures through its CLI JSON: iterative_solver_iterations, final
- * residual, phase seconds; app/half_cli.F90:306-349). */
+/* Diagnostics of the last device call on this context (solve, H/S
+ * application or force); the reference reports the solver figures through its
+ * CLI JSON: iterative_solver_iterations, final residual, phase seconds
+ * (app/half_cli.F90:306-349).  Event times are measured on the library's
+ * CUDA stream. */
 typedef struct half_solve_info_v1 {
   uint32_t struct_size;        /* set to sizeof(half_solve_info_v1) */
   int32_t iterations;          /* ACC iterations (all phases) */
@@ -45,7 +47,15 @@ typedef struct half_solve_info_v1 {
   double setup_ms;             /* basis, projectors, operator tables */
   double solve_ms;             /* iterations through eigenpairs */
   double operator_ms;          /* time inside H/S applications */
-  uint64_t reserved[6];
+  double device_ms;            /* CUDA-event span on the library stream */
+  double local_ms;             /* CUDA-event time of the local-operator kernels */
+  double local_bytes;          /* their algorithmic bytes (FFT-path figure per band) */
+  int64_t local_columns;       /* band columns through the local operator */
+  int64_t kernel_launches;     /* library kernels launched by the call */
+  double sweep_ms;             /* CUDA-event time of whole H/S applications */
+  int64_t sweep_columns;       /* band columns of those applications */
+  double adjoint_ms;           /* CUDA-event time of the force adjoint (GEMM + epilogue) */
+  uint64_t reserved[4];
 } half_solve_info_v1;
 int half_get_last_solve_info(half_handle handle, half_solve_info_v1 *info,
                              char *error, int error_capacity);

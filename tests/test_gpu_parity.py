@@ -80,18 +80,23 @@ def test_index_range_solver(si2, oracle_system):
     assert vec.shape == (op.basis.npw, 8)
 
 
-def test_acc_fp64_matches_oracle_acc(si2, oracle_system):
-    """Same controls, same algorithm: the ACC iterates match the oracle's."""
+def test_acc_fp64_iterates_match_oracle_acc(hfo2, oracle_system):
+    """Same controls, same algorithm: after a fixed number of unconverged
+    iterations the Ritz values match the oracle's restatement.  The
+    monoclinic cell has no symmetry-degenerate levels, so the iterates are
+    well defined (in degenerate spectra the choice of basis inside a
+    degenerate eigenspace differs between eigensolver libraries)."""
     from oracle import hamiltonian as H, acc
-    op = H.prepare(oracle_system("si2", si2))
-    ref = acc.solve_acc(op, 8, tol=1e-4, max_iterations=40)
-    with ctx_for(si2) as ctx:
-        ctx.set_acc(tol=1e-4, max_iterations=40)
-        eg, _, smin, smax = ctx.solve((0, 0, 0), 8)
+    op = H.prepare(oracle_system("hfo2", hfo2))
+    ref = acc.solve_acc(op, 16, tol=1e-12, max_iterations=8)
+    with ctx_for(hfo2) as ctx:
+        ctx.set_acc(tol=1e-12, max_iterations=8)
+        eg, _, smin, smax = ctx.solve((0, 0, 0), 16)
         info = ctx.info()
     assert smin == -1.0 and smax == -1.0
-    assert info["iterations"] == ref.iterations
-    assert np.abs(eg - ref.eigenvalues).max() <= 1e-10
+    assert info["iterations"] == ref.iterations == 8
+    print("acc iterate parity", np.abs(eg - ref.eigenvalues).max())
+    assert np.abs(eg - ref.eigenvalues).max() <= 1e-9
 
 
 def test_acc_fp64_converges_to_dense(si2, oracle_system):
@@ -119,14 +124,27 @@ def test_acc_mixed_converges_to_dense(si2, oracle_system):
     assert np.abs(eg - w).max() <= 1e-8
 
 
-def test_mapped_solve_reverse_order(si2):
+def test_mapped_solve_reverse_order(si2, oracle_system):
+    """half_solve_kpoint_mapped returns the eigenvectors in the host's G order:
+    undoing a reversed host order gives eigenvectors of the oracle's dense
+    H, S in HALF order (degenerate levels make a row-by-row comparison of two
+    separate solves meaningless)."""
+    from oracle import hamiltonian as H
+    op = H.prepare(oracle_system("si2", si2))
+    h, s = H.assemble_dense(op)
     with ctx_for(si2, solver="evd") as ctx:
         g, _ = ctx.basis((0, 0, 0))
-        e0, v0, _, _ = ctx.solve((0, 0, 0), 8, vectors=True)
+        e0, _, _, _ = ctx.solve((0, 0, 0), 8)
         rev = g[::-1].copy()
         e1, v1, _, _ = ctx.solve_mapped((0, 0, 0), 8, rev)
-    assert np.array_equal(e0, e1)
-    assert np.array_equal(v1, v0[::-1])
+        with pytest.raises(halfb200.HalfError) as ei:
+            ctx.solve_mapped((0, 0, 0), 8, np.concatenate([rev[:1], rev[:-1]]))
+        assert ei.value.status == halfb200.HALF_ERROR_INVALID_ARGUMENT
+    assert np.abs(e0 - e1).max() <= 1e-12
+    v = v1[::-1]
+    res = h @ v - (s @ v) * e1[None, :]
+    assert np.abs(res).max() <= 1e-9
+    assert np.abs(v.conj().T @ s @ v - np.eye(8)).max() <= 1e-10
 
 
 def test_nonlocal_forces_match_oracle(si2, oracle_system):
