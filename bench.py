@@ -40,12 +40,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="hfo2")
-    p.add_argument("--tol", type=float, default=1e-4, help="ACC residual tolerance (eV)")
+    p.add_argument("--tol", type=float, default=3e-5,
+                   help="ACC residual tolerance (eV); 3e-5 puts |d eps| below 1e-8 eV on this workload")
     p.add_argument("--max-iter", type=int, default=2000)
     p.add_argument("--block", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-mode comparison run")
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    p.add_argument("--no-check", action="store_true",
+                   help="skip the dense FP64 reference eigenvalues (profiling runs; |d eps| reported as null)")
     return p.parse_args()
 
 
@@ -250,8 +253,11 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
 
     # ---- FP64 dense reference eigenvalues (untimed)
-    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="evd") as dctx:
-        dense = [dctx.solve(k, w.nbands)[0] for k in kpts]
+    if args.no_check:
+        dense = None
+    else:
+        with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="evd") as dctx:
+            dense = [dctx.solve(k, w.nbands)[0] for k in kpts]
 
     def run_mode(ctx, precision, steps, warmup):
         ctx.set_acc(tol=args.tol, max_iterations=args.max_iter, block_size=args.block, precision=precision)
@@ -271,7 +277,8 @@ def main():
                 dev_ms.append(max_over_ranks(inf["device_ms"]))
                 wall_ms.append(max_over_ranks((t1 - t0) * 1e3))
                 infos.append(inf)
-                errs.append(max(float(np.abs(e - d).max()) for e, d in zip(eig, dense)))
+                if dense is not None:
+                    errs.append(max(float(np.abs(e - d).max()) for e, d in zip(eig, dense)))
         return dev_ms, wall_ms, infos, errs
 
     with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
@@ -329,11 +336,11 @@ def main():
                                f"{w.nbands} bands, PBE, MIMIC_US D_ij", "tol_eV": args.tol,
                    "block": args.block, "kpoints_per_rank": nk, "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"k-point ownership x{world}" if world > 1 else "single GPU"},
-        "max_abs_d_eps_eV": max(errs), "iterations": int(statistics.mean(i["iterations"] for i in infos)),
+        "max_abs_d_eps_eV": max(errs) if errs else None, "iterations": int(statistics.mean(i["iterations"] for i in infos)),
         "fp64_refinement_iterations": int(statistics.mean(i["fp64_iterations"] for i in infos)),
         "wall_ms_per_step": statistics.mean(wall_ms),
         "fp64_mode": ({"ms_per_k": statistics.mean(fp64[0]) / nk_total, "iterations": fp64_iters,
-                       "max_abs_d_eps_eV": max(fp64[3])} if fp64 else None),
+                       "max_abs_d_eps_eV": max(fp64[3]) if fp64[3] else None} if fp64 else None),
         "mixed_speedup_vs_fp64": (statistics.mean(fp64[0]) / ms_step) if fp64 else None,
         "force_adjoint_ms": statistics.mean(adj), "forward_sweep_ms": statistics.mean(sweep),
         "force_over_sweep": statistics.mean(adj) / statistics.mean(sweep),

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 
 #include "blas.h"
 #include "context.h"
@@ -162,6 +163,31 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Phase tracer (environment HALF_TRACE=1): synchronises the stream at each
+// mark and attributes the elapsed host time to the named phase; the totals go
+// to stderr at the end of the solve.  Off by default (no synchronisation).
+struct Tracer {
+  bool on = std::getenv("HALF_TRACE") != nullptr;
+  cudaStream_t s = nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  std::vector<std::pair<const char*, double>> acc;
+  void mark(const char* name) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    double d = ms_since(t);
+    t = std::chrono::steady_clock::now();
+    for (auto& p : acc)
+      if (p.first == name) { p.second += d; return; }
+    acc.push_back({name, d});
+  }
+  void report(int iters) {
+    if (!on) return;
+    std::fprintf(stderr, "HALF trace (%d iterations):", iters);
+    for (auto& p : acc) std::fprintf(stderr, " %s=%.2fms", p.first, p.second);
+    std::fprintf(stderr, "\n");
+  }
+};
+
 // FP64 small dense solves on the context's cuSOLVER handle; the status words
 // stay on the device and are read with the next residual norms.
 struct SmallSolver {
@@ -262,6 +288,8 @@ struct AccRun {
   int n, m, chunk;
   double op_ms = 0;
   long long op_cols = 0;
+  Tracer* tr = nullptr;
+  void mark(const char* s) { if (tr) tr->mark(s); }
 
   void apply(const C* x, C* hx, C* sx, int nb) {
     auto t0 = std::chrono::steady_clock::now();
@@ -317,6 +345,7 @@ struct AccRun {
     HALF_CUDA(cudaMemcpyAsync(norms.data(), sc.norms.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
     HALF_CUDA(cudaMemcpyAsync(infos, ss.info.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
     HALF_CUDA(cudaStreamSynchronize(rt.stream));
+    mark("residual");
     if (infos[0] != 0) fail(kInternal, "ACC correction metric eigensolve failed (info " + std::to_string(infos[0]) + ")");
     if (infos[1] != 0) fail(kInternal, "ACC small generalized eigensolve failed (info " + std::to_string(infos[1]) + ")");
     double mx = 0;
@@ -333,12 +362,15 @@ struct AccRun {
                                                                        blk.P.get());
     ++rt.prof.launches;
     HALF_LAUNCH("precondition");
+    mark("precondition");
     apply(blk.P.get(), blk.HP.get(), blk.SP.get(), m);
+    mark("apply");
     // S-orthogonalise against X
     gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.SP.get(), n, zero, blk.small.get(), m);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.x(), n, blk.small.get(), m, one, blk.P.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.hx(), n, blk.small.get(), m, one, blk.HP.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.sx(), n, blk.small.get(), m, one, blk.SP.get(), n);
+    mark("orth_gemm");
     // S-metric normalisation
     double2* metric = sc.metric.get();
     if constexpr (sizeof(R) == 8) {
@@ -349,13 +381,16 @@ struct AccRun {
                                                                                                (long long)m * m);
       ++rt.prof.launches;
     }
+    mark("metric_gemm");
     ss.heevd(metric, m, sc.mu.get());
+    mark("heevd");
     scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14);
     ++rt.prof.launches;
     to_r(metric, m, blk.small.get(), m, m, m);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.P.get(), n, blk.small.get(), m, zero, blk.PU.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HP.get(), n, blk.small.get(), m, zero, blk.HPU.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.SP.get(), n, blk.small.get(), m, zero, blk.SPU.get(), n);
+    mark("metric_rot");
     // Rayleigh-Ritz on Z = [X PU]
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
@@ -366,7 +401,9 @@ struct AccRun {
       project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.hx(), blk.HPU.get(), tmp2m.get(), hs);
       project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.sx(), blk.SPU.get(), tmp2m.get(), ssb);
     }
+    mark("rr_gemm");
     ss.hegvd(hs, ssb, 2 * m, sc.w.get());
+    mark("hegvd");
     to_r(hs, 2 * m, blk.Y.get(), 2 * m, 2 * m, m);
     const C* ytop = blk.Y.get();
     const C* ybot = blk.Y.get() + m;
@@ -378,14 +415,15 @@ struct AccRun {
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, 2 * m, zero, blk.SX[nx].get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.SPU.get(), n, ybot, 2 * m, one, blk.SX[nx].get(), n);
     blk.cur = nx;
+    mark("rr_rot");
   }
 };
 
 }  // namespace
 
-void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out) {
+void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out, SolveInfo& info) {
   auto t_start = std::chrono::steady_clock::now();
-  Runtime& rt = *ctx.rt;
+  Runtime& rt = *ks.rt;
   const int n = int(ks.basis.npw());
   const int m = nbands;
   if (m < 1 || m > n) fail(kInvalidArgument, "invalid ACC target band count");
@@ -416,7 +454,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   Blocks<double> b64;
   b64.allocate(n, m);
   DeviceBuffer<double2> tmp64(size_t(4) * m * m);
+  Tracer tracer;
+  tracer.s = rt.stream;
   AccRun<double> run64{ctx, ks, rt, b64, sc, ss, tmp64, n, m, cfg.block};
+  run64.tr = &tracer;
 
   if (mixed) {
     // ---------------- FP32 phase
@@ -424,6 +465,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     b32.allocate(n, m);
     DeviceBuffer<float2> tmp32(size_t(4) * m * m);
     AccRun<float> run32{ctx, ks, rt, b32, sc, ss, tmp32, n, m, cfg.block};
+    run32.tr = &tracer;
     init_states_kernel<float2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b32.x(), n, n, m, sc.idx.get());
     ++rt.prof.launches;
     run32.apply(b32.x(), b32.hx(), b32.sx(), m);
@@ -483,14 +525,15 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
                               rt.stream));
   }
   HALF_CUDA(cudaStreamSynchronize(rt.stream));
-  ctx.last.iterations = iter;
-  ctx.last.fp64_iterations = fp64_iter;
-  ctx.last.converged = converged ? 1 : 0;
-  ctx.last.max_residual = max_res;
-  ctx.last.npw = n;
-  ctx.last.operator_columns = op_cols;
-  ctx.last.operator_ms = op_ms;
-  ctx.last.solve_ms = ms_since(t_start);
+  tracer.report(iter);
+  info.iterations = iter;
+  info.fp64_iterations = fp64_iter;
+  info.converged = converged ? 1 : 0;
+  info.max_residual = max_res;
+  info.npw = n;
+  info.operator_columns = op_cols;
+  info.operator_ms = op_ms;
+  info.solve_ms = ms_since(t_start);
   if (!converged && max_res > std::max(100.0 * cfg.tol, 1e-2))
     std::fprintf(stderr, "HALF ACC warning: stopped after %d iterations; max residual=%12.4E\n", cfg.max_iter, max_res);
 }

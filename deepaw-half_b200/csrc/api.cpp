@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 
 #include "../../include/half_b200.h"
 #include "context.h"
@@ -137,48 +138,72 @@ int create_context(const std::string& charge, const std::string& potential, doub
 }
 
 // Event accounting around one device call (solve, H/S application, force).
-void begin_call(Context& ctx) {
-  Profile& pf = ctx.rt->prof;
+void begin_call(Runtime& rt) {
+  Profile& pf = rt.prof;
   pf.reset();
-  HALF_CUDA(cudaEventRecord(pf.a, ctx.rt->stream));
+  HALF_CUDA(cudaEventRecord(pf.a, rt.stream));
 }
 
-void end_call(Context& ctx) {
-  Profile& pf = ctx.rt->prof;
-  HALF_CUDA(cudaEventRecord(pf.b, ctx.rt->stream));
+void end_call(Runtime& rt, SolveInfo& info) {
+  Profile& pf = rt.prof;
+  HALF_CUDA(cudaEventRecord(pf.b, rt.stream));
   HALF_CUDA(cudaEventSynchronize(pf.b));
   float ms = 0;
   HALF_CUDA(cudaEventElapsedTime(&ms, pf.a, pf.b));
-  ctx.last.device_ms = ms;
-  ctx.last.local_ms = pf.local_ms;
-  ctx.last.local_bytes = pf.local_bytes;
-  ctx.last.local_columns = pf.local_columns;
-  ctx.last.launches = pf.launches;
-  ctx.last.sweep_ms = pf.sweep_ms;
-  ctx.last.sweep_columns = pf.sweep_columns;
-  ctx.last.adjoint_ms = pf.adjoint_ms;
+  info.device_ms = ms;
+  info.local_ms = pf.local_ms;
+  info.local_bytes = pf.local_bytes;
+  info.local_columns = pf.local_columns;
+  info.launches = pf.launches;
+  info.sweep_ms = pf.sweep_ms;
+  info.sweep_columns = pf.sweep_columns;
+  info.adjoint_ms = pf.adjoint_ms;
 }
 
-// Solve one k point with the context's solver; out holds device vectors.
-void solve_one(Context& ctx, const double k[3], int nbands, bool want_vectors, SolveOutput& out,
-               std::unique_ptr<KOperatorSet>* keep = nullptr) {
+// Solve one k point with the context's solver on runtime rt; out holds device vectors.
+void solve_one(Context& ctx, Runtime& rt, const double k[3], int nbands, bool want_vectors, SolveOutput& out,
+               SolveInfo& info, std::unique_ptr<KOperatorSet>* keep = nullptr) {
   auto t0 = std::chrono::steady_clock::now();
   if (!finite3(k)) fail(kInvalidArgument, "k point must be finite");
-  begin_call(ctx);
+  info = SolveInfo();
+  begin_call(rt);
   bool mixed = ctx.solver == HALF_SOLVER_ACC && ctx.acc.precision == kMixed;
-  auto ks = prepare_operator(ctx, k, true, mixed);
+  auto ks = prepare_operator(ctx, rt, k, true, mixed);
   double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (nbands < 1 || nbands > ks->basis.npw()) fail(kInvalidArgument, "invalid requested band count");
   switch (ctx.solver) {
-    case HALF_SOLVER_ACC: solve_acc(ctx, *ks, nbands, want_vectors, out); break;
-    case HALF_SOLVER_EVD: solve_dense(ctx, *ks, nbands, false, want_vectors, out); ctx.last = SolveInfo(); break;
-    case HALF_SOLVER_VASP: solve_dense(ctx, *ks, nbands, true, want_vectors, out); ctx.last = SolveInfo(); break;
+    case HALF_SOLVER_ACC: solve_acc(ctx, *ks, nbands, want_vectors, out, info); break;
+    case HALF_SOLVER_EVD: solve_dense(ctx, *ks, nbands, false, want_vectors, out); break;
+    case HALF_SOLVER_VASP: solve_dense(ctx, *ks, nbands, true, want_vectors, out); break;
     default: fail(kUnavailable, "the EVJ (Jacobi) dense solver is not built in this B200 library; use EVD, VASP or ACC");
   }
-  ctx.last.setup_ms = setup_ms;
-  ctx.last.npw = ks->basis.npw();
-  end_call(ctx);
+  info.setup_ms = setup_ms;
+  info.npw = ks->basis.npw();
+  end_call(rt, info);
   if (keep) *keep = std::move(ks);
+}
+
+void solve_one(Context& ctx, const double k[3], int nbands, bool want_vectors, SolveOutput& out,
+               std::unique_ptr<KOperatorSet>* keep = nullptr) {
+  solve_one(ctx, *ctx.rt, k, nbands, want_vectors, out, ctx.last, keep);
+}
+
+void accumulate(SolveInfo& total, const SolveInfo& s, bool first) {
+  total.iterations += s.iterations;
+  total.fp64_iterations += s.fp64_iterations;
+  total.converged = (first ? 1 : total.converged) & s.converged;
+  total.operator_columns += s.operator_columns;
+  total.max_residual = std::max(total.max_residual, s.max_residual);
+  total.setup_ms += s.setup_ms;
+  total.solve_ms += s.solve_ms;
+  total.operator_ms += s.operator_ms;
+  total.npw += s.npw;
+  total.local_ms += s.local_ms;
+  total.local_bytes += s.local_bytes;
+  total.local_columns += s.local_columns;
+  total.launches += s.launches;
+  total.sweep_ms += s.sweep_ms;
+  total.sweep_columns += s.sweep_columns;
 }
 
 }  // namespace
@@ -368,7 +393,7 @@ int half_assemble_hs(half_handle handle, const double kpoint[3], int64_t ld, HAL
   if (!h || !s) { export_error("H and S output pointers are required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
   return guarded(error, cap, [&]() -> int {
     if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
-    auto ks = prepare_operator(*ctx, kpoint, true, false);
+    auto ks = prepare_operator(*ctx, *ctx->rt, kpoint, true, false);
     long long n = ks->basis.npw();
     if (ld < n) fail(kCapacity, "matrix leading dimension is too small");
     DeviceBuffer<double2> dh((size_t)n * n), ds((size_t)n * n);
@@ -392,7 +417,7 @@ int half_apply_hs(half_handle handle, const double kpoint[3], int nstates, int64
   return guarded(error, cap, [&]() -> int {
     if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
     bool fp32 = ctx->acc.precision == kMixed;
-    auto ks = prepare_operator(*ctx, kpoint, true, fp32);
+    auto ks = prepare_operator(*ctx, *ctx->rt, kpoint, true, fp32);
     long long n = ks->basis.npw();
     if (ld < n) fail(kCapacity, "state leading dimension is too small");
     cudaStream_t st = ctx->rt->stream;
@@ -400,9 +425,9 @@ int half_apply_hs(half_handle handle, const double kpoint[3], int nstates, int64
     HALF_CUDA(cudaMemcpy2DAsync(x.get(), n * sizeof(double2), psi, ld * sizeof(double2), n * sizeof(double2), nstates,
                                 cudaMemcpyHostToDevice, st));
     ctx->last = SolveInfo();
-    begin_call(*ctx);
+    begin_call(*ctx->rt);
     apply_hs<double>(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
-    end_call(*ctx);
+    end_call(*ctx->rt, ctx->last);
     HALF_CUDA(cudaMemcpy2DAsync(hpsi, ld * sizeof(double2), hx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
                                 cudaMemcpyDeviceToHost, st));
     HALF_CUDA(cudaMemcpy2DAsync(spsi, ld * sizeof(double2), sx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
@@ -562,28 +587,58 @@ int half_solve_kpoints(half_handle handle, int nk, const double* kpoints, int nb
     return HALF_ERROR_INVALID_ARGUMENT;
   }
   return guarded(error, cap, [&]() -> int {
-    SolveInfo total;
-    for (int ik = 0; ik < nk; ++ik) {
-      SolveOutput out;
-      solve_one(*ctx, kpoints + 3 * ik, nbands, false, out);
-      std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues + (size_t)ik * nbands);
-      total.iterations += ctx->last.iterations;
-      total.fp64_iterations += ctx->last.fp64_iterations;
-      total.converged = (ik == 0 ? 1 : total.converged) & ctx->last.converged;
-      total.operator_columns += ctx->last.operator_columns;
-      total.max_residual = std::max(total.max_residual, ctx->last.max_residual);
-      total.setup_ms += ctx->last.setup_ms;
-      total.solve_ms += ctx->last.solve_ms;
-      total.operator_ms += ctx->last.operator_ms;
-      total.npw += ctx->last.npw;
-      total.device_ms += ctx->last.device_ms;
-      total.local_ms += ctx->last.local_ms;
-      total.local_bytes += ctx->last.local_bytes;
-      total.local_columns += ctx->last.local_columns;
-      total.launches += ctx->last.launches;
-      total.sweep_ms += ctx->last.sweep_ms;
-      total.sweep_columns += ctx->last.sweep_columns;
+    // k points are independent: up to `workers` of them run concurrently, each
+    // on its own stream with its own cuBLAS/cuSOLVER handles, so one k point's
+    // host-side solver latency overlaps another's device work.
+    const int workers = std::max(1, std::min(nk, ctx->kpoint_workers));
+    while ((int)ctx->workers.size() < workers - 1) ctx->workers.push_back(std::make_unique<Runtime>());
+    std::vector<SolveInfo> infos(nk);
+    std::vector<std::string> errors(workers);
+    std::vector<int> codes(workers, 0);
+    HALF_CUDA(cudaDeviceSynchronize());
+    cudaEvent_t t0;
+    HALF_CUDA(cudaEventCreate(&t0));
+    HALF_CUDA(cudaEventRecord(t0, ctx->rt->stream));
+    std::vector<cudaEvent_t> ends(workers);
+    for (auto& e : ends) HALF_CUDA(cudaEventCreate(&e));
+    auto body = [&](int w) {
+      Runtime& rt = w == 0 ? *ctx->rt : *ctx->workers[w - 1];
+      try {
+        for (int ik = w; ik < nk; ik += workers) {
+          SolveOutput out;
+          solve_one(*ctx, rt, kpoints + 3 * ik, nbands, false, out, infos[ik]);
+          std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues + (size_t)ik * nbands);
+        }
+      } catch (const Error& e) {
+        codes[w] = e.status;
+        errors[w] = e.what();
+      } catch (const std::exception& e) {
+        codes[w] = HALF_ERROR_INTERNAL;
+        errors[w] = e.what();
+      }
+      cudaEventRecord(ends[w], rt.stream);
+    };
+    if (workers == 1) {
+      body(0);
+    } else {
+      std::vector<std::thread> pool;
+      for (int w = 0; w < workers; ++w) pool.emplace_back(body, w);
+      for (auto& t : pool) t.join();
     }
+    float span = 0;
+    for (int w = 0; w < workers; ++w) {
+      HALF_CUDA(cudaEventSynchronize(ends[w]));
+      float ms = 0;
+      HALF_CUDA(cudaEventElapsedTime(&ms, t0, ends[w]));
+      span = std::max(span, ms);
+      cudaEventDestroy(ends[w]);
+    }
+    cudaEventDestroy(t0);
+    for (int w = 0; w < workers; ++w)
+      if (codes[w] != 0) fail(codes[w], errors[w]);
+    SolveInfo total;
+    for (int ik = 0; ik < nk; ++ik) accumulate(total, infos[ik], ik == 0);
+    total.device_ms = span;   // wall span on the device of the whole batch
     ctx->last = total;
     return HALF_SUCCESS;
   });
@@ -616,7 +671,7 @@ int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands,
   }
   return guarded(error, cap, [&]() -> int {
     if (!finite3(kpoint)) fail(kInvalidArgument, "k point must be finite");
-    auto ks = prepare_operator(*ctx, kpoint, true, false);
+    auto ks = prepare_operator(*ctx, *ctx->rt, kpoint, true, false);
     long long n = ks->basis.npw();
     if (ld < n) fail(kCapacity, "eigenvector leading dimension is too small");
     cudaStream_t st = ctx->rt->stream;
@@ -624,9 +679,9 @@ int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands,
     HALF_CUDA(cudaMemcpy2DAsync(dv.get(), n * sizeof(double2), vectors, ld * sizeof(double2), n * sizeof(double2),
                                 nbands, cudaMemcpyHostToDevice, st));
     ctx->last = SolveInfo();
-    begin_call(*ctx);
+    begin_call(*ctx->rt);
     nonlocal_forces_device(*ctx, *ks, dv.get(), n, nbands, eigenvalues, occupations, kweight, forces);
-    end_call(*ctx);
+    end_call(*ctx->rt, ctx->last);
     return HALF_SUCCESS;
   });
 }
@@ -662,7 +717,7 @@ extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoint
     int nions = ctx->crystal.nions();
     std::fill(forces, forces + 3 * nions, 0.0);
     for (int ik = 0; ik < nk; ++ik) {
-      auto ks = prepare_operator(*ctx, kpoints + 3 * ik, true, false);
+      auto ks = prepare_operator(*ctx, *ctx->rt, kpoints + 3 * ik, true, false);
       nonlocal_forces_device(*ctx, *ks, outs[ik].dvectors.get(), ks->basis.npw(), nbands, eig.data() + (size_t)ik * nbands,
                              occ.data() + (size_t)ik * nbands, kweights[ik], forces);
     }

@@ -105,6 +105,8 @@ struct Context {
   std::vector<double> request_positions;
 
   std::unique_ptr<Runtime> rt;
+  std::vector<std::unique_ptr<Runtime>> workers;   // extra streams for concurrent k points
+  int kpoint_workers = 4;
   DeviceBuffer<double> veff;           // C order, eV
   std::vector<SpeciesDevice> species;
 
@@ -123,6 +125,7 @@ template <typename R>
 struct KOperator;   // hs.cu
 
 struct KOperatorSet {
+  Runtime* rt = nullptr;                      // stream and handles the operator runs on
   Basis basis;
   int np = 0;                                 // projector columns (all species)
   std::unique_ptr<KOperator<double>> op64;
@@ -131,7 +134,7 @@ struct KOperatorSet {
   ~KOperatorSet();
 };
 
-std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, const double k[3], bool fp64, bool fp32);
+std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const double k[3], bool fp64, bool fp32);
 
 // H/S application on device blocks (column-major, leading dimension ld).
 template <typename R>
@@ -145,7 +148,7 @@ struct SolveOutput {
   double overlap_min = -1, overlap_max = -1;
   DeviceBuffer<double2> dvectors;    // device copy (kept for forces)
 };
-void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out);
+void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out, SolveInfo& info);
 void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, bool want_vectors, SolveOutput& out);
 void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s);   // device N x N
 

@@ -83,7 +83,7 @@ __global__ void to_complex_kernel(const double* in, double2* out, long long n) {
 }  // namespace
 
 void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s) {
-  Runtime& rt = *ctx.rt;
+  Runtime& rt = *ks.rt;
   cudaStream_t st = rt.stream;
   const Basis& b = ks.basis;
   const int n = int(b.npw());
@@ -141,7 +141,7 @@ void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s) {
 }
 
 void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, bool want_vectors, SolveOutput& out) {
-  Runtime& rt = *ctx.rt;
+  Runtime& rt = *ks.rt;
   cudaStream_t st = rt.stream;
   const int n = int(ks.basis.npw());
   if (nbands < 1 || nbands > n) fail(kInvalidArgument, "invalid requested band count");

@@ -104,7 +104,7 @@ __global__ void force_epilogue_kernel(const double2* __restrict__ cc, int np, in
 
 void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec, long long ld, int nb, const double* eig,
                             const double* occ, double kweight, double* forces_host) {
-  Runtime& rt = *ctx.rt;
+  Runtime& rt = *ks.rt;
   cudaStream_t st = rt.stream;
   const int npw = int(ks.basis.npw()), np = ks.np;
   const int nions = ctx.crystal.nions();

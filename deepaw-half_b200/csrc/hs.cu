@@ -285,10 +285,10 @@ HostGeom plane_geometry(const Basis& b, const AxisPlan& ax, const AxisPlan& ay, 
 }
 
 template <typename R>
-void fill_operator(Context& ctx, const Basis& basis, const HostGeom& hg, const DeviceBuffer<double2>& B64, int np,
+void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom& hg, const DeviceBuffer<double2>& B64, int np,
                    const std::vector<int>& cb, const std::vector<int>& ca, const std::vector<int>& cn,
                    const std::vector<int>& cd, const std::vector<int>& cq, KOperator<R>& op) {
-  cudaStream_t s = ctx.rt->stream;
+  cudaStream_t s = rt.stream;
   op.npw = int(basis.npw());
   op.n1 = basis.shape[0]; op.n2 = basis.shape[1]; op.n3 = basis.shape[2];
   op.ax = make_axis_plan(op.n1); op.ay = make_axis_plan(op.n2); op.az = make_axis_plan(op.n3);
@@ -344,13 +344,14 @@ void fill_operator(Context& ctx, const Basis& basis, const HostGeom& hg, const D
 
 }  // namespace
 
-std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, const double k[3], bool fp64, bool fp32) {
+std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const double k[3], bool fp64, bool fp32) {
   auto ks = std::make_unique<KOperatorSet>();
+  ks->rt = &rt;
   ks->basis = build_basis(ctx.crystal, ctx.charge.shape, ctx.encut, k);
   const Basis& basis = ks->basis;
   const int npw = int(basis.npw());
   if (npw < 1) fail(kInvalidArgument, "empty plane-wave basis");
-  cudaStream_t s = ctx.rt->stream;
+  cudaStream_t s = rt.stream;
   AxisPlan ax = make_axis_plan(basis.shape[0]), ay = make_axis_plan(basis.shape[1]), az = make_axis_plan(basis.shape[2]);
   HostGeom hg = plane_geometry(basis, ax, ay, az);
   // projector columns: species-major, atom-major, then (channel, m)
@@ -401,11 +402,11 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, const double k[3], 
   }
   if (fp64) {
     ks->op64 = std::make_unique<KOperator<double>>();
-    fill_operator<double>(ctx, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op64);
+    fill_operator<double>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op64);
   }
   if (fp32) {
     ks->op32 = std::make_unique<KOperator<float>>();
-    fill_operator<float>(ctx, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op32);
+    fill_operator<float>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op32);
   }
   HALF_CUDA(cudaStreamSynchronize(s));
   return ks;
@@ -433,7 +434,7 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
               int chunk) {
   using C = cplx_t<R>;
   KOperator<R>& op = pick<R>(ks);
-  Runtime& rt = *ctx.rt;
+  Runtime& rt = *ks.rt;
   cudaStream_t s = rt.stream;
   if (nb <= 0) return;
   chunk = std::max(1, std::min(chunk, nb));

@@ -8,7 +8,9 @@
 //   which also provides dD/dR and symmetrises both); the GPU D-only variant
 //   src/half_cuda_uspp.cuf:124-195 is the same algorithm without symmetrising.
 // All full-box transforms use the library's own shared-memory FFT engine.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "context.h"
 
@@ -593,6 +595,7 @@ void build_dij_device(Context& ctx, bool gradient) {
 
 void Context::initialize() {
   if (!rt) rt = std::make_unique<Runtime>();
+  if (const char* w = std::getenv("HALF_KPOINT_STREAMS")) kpoint_workers = std::max(1, std::atoi(w));
   for (int j = 0; j < 3; ++j) make_fft_plan(charge.shape[j]);   // validates the box
   species.clear();
   species.resize(pots.size());
