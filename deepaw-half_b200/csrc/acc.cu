@@ -18,18 +18,24 @@
 //   cuBLAS/cuSOLVER handle lives on the context stream, and the only
 //   host<->device traffic per iteration is the m residual norms plus the
 //   solver status words (one synchronisation, as in the reference);
+// * with the library's own small eigensolver (eig.cu, HALF_SMALL_EIG=own) the
+//   correction metric is Jacobi-scaled before its eigendecomposition; the
+//   normalised directions span the same space, so the Ritz values are those
+//   of the reference up to rounding;
 // * precision MIXED runs the iterations on FP32 blocks (FP32 operator,
 //   BF16x9 tensor-core GEMMs when cuBLAS provides them, FP64 small
 //   eigensolves) until the residual reaches the FP32 regime, then promotes X
 //   and finishes with FP64 iterations (one FP64 operator sweep re-creates
 //   H X and S X exactly before the first FP64 Rayleigh-Ritz).
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
 
 #include "blas.h"
 #include "context.h"
+#include "eig.h"
 
 namespace hb {
 
@@ -128,11 +134,30 @@ __global__ void precondition_kernel(const C* __restrict__ hx, const C* __restric
 }
 
 // U[:, j] /= sqrt(max(mu_j, floor))  (src/half_cuda_iterative_solver.cuf:66-77)
-__global__ void scale_columns_kernel(double2* u, int m, const double* mu, double floor_value) {
+// u[:, j] /= sqrt(max(mu_j, floor)); rows scaled by dsc[i] when the metric
+// was Jacobi-scaled (dsc == nullptr: no row scaling)
+__global__ void scale_columns_kernel(double2* u, int m, const double* mu, double floor_value, const double* dsc) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m * m) return;
-  int j = t / m;
-  u[t] = cscale(u[t], 1.0 / sqrt(fmax(mu[j], floor_value)));
+  int j = t / m, i = t - j * m;
+  u[t] = cscale(u[t], (dsc ? dsc[i] : 1.0) / sqrt(fmax(mu[j], floor_value)));
+}
+
+// Jacobi scaling of the correction metric M = P^H S P for the library's own
+// small eigensolver: M <- D M D with D = diag(M)^-1/2.  P D U' spans what
+// P U spans, so the Rayleigh-Ritz step sees the same space; the spectrum of
+// D M D is O(1), whereas M itself carries one tiny eigenvalue per nearly
+// converged band (P columns of the size of their residuals), which the
+// bisection / inverse-iteration solver would treat as one large cluster.
+__global__ void metric_diag_kernel(const double2* __restrict__ M, int m, double* __restrict__ dsc) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) dsc[j] = 1.0 / sqrt(fmax(M[(size_t)j * m + j].x, DBL_MIN));
+}
+__global__ void metric_scale_kernel(double2* __restrict__ M, int m, const double* __restrict__ dsc) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m * m) return;
+  int j = t / m, i = t - j * m;
+  M[t] = cscale(M[t], dsc[i] * dsc[j]);
 }
 
 template <typename A, typename B>
@@ -190,13 +215,25 @@ struct Tracer {
 
 // FP64 small dense solves on the context's cuSOLVER handle; the status words
 // stay on the device and are read with the next residual norms.
+// By default cuSOLVER zheevd/zhegvd, as the reference does; environment
+// HALF_SMALL_EIG=own selects the library's device-resident solvers (eig.cu).
 struct SmallSolver {
   Runtime& rt;
   int m;
   DeviceBuffer<double2> work;
-  DeviceBuffer<int> info;   // [0] metric heevd, [1] RR hegvd
+  DeviceBuffer<int> info;   // [0] metric heevd, [1] RR hegvd, [2] RR Cholesky (own solver)
   int lw_ev = 0, lw_gv = 0;
+  bool own = true;
+  SmallEigen eig;
   SmallSolver(Runtime& r, int m_, double2* a, double2* b, double* w) : rt(r), m(m_) {
+    const char* sel = std::getenv("HALF_SMALL_EIG");
+    own = sel && std::string(sel) == "own";
+    info.resize(3);
+    info.zero(rt.stream);
+    if (own) {
+      eig.reserve(rt, 2 * m);
+      return;
+    }
     int l1 = 0, l2 = 0, l3 = 0;
     cusolver_check(cusolverDnZheevd_bufferSize(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m,
                                                reinterpret_cast<cuDoubleComplex*>(a), m, w, &l1),
@@ -210,23 +247,29 @@ struct SmallSolver {
                                                reinterpret_cast<cuDoubleComplex*>(b), m, w, &l3),
                    "zhegvd buffer");
     work.resize(size_t(std::max({l1, l2, l3, 1})));
-    info.resize(2);
-    info.zero(rt.stream);
     lw_ev = l1;
     lw_gv = std::max(l2, l3);
   }
+  // all n eigenpairs of a (n x n)
   void heevd(double2* a, int n, double* w) {
+    if (own) { eig.heev(rt, a, n, n, w, info.get()); return; }
     cusolver_check(cusolverDnZheevd(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n,
                                     reinterpret_cast<cuDoubleComplex*>(a), n, w,
                                     reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()), info.get()),
                    "zheevd");
   }
-  void hegvd(double2* a, double2* b, int n, double* w) {
+  // generalized problem of order n; the nev lowest eigenvectors are wanted
+  void hegvd(double2* a, double2* b, int n, double* w, int nev) {
+    if (own) { eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2); return; }
     cusolver_check(cusolverDnZhegvd(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
                                     n, reinterpret_cast<cuDoubleComplex*>(a), n, reinterpret_cast<cuDoubleComplex*>(b),
                                     n, w, reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()),
                                     info.get() + 1),
                    "zhegvd");
+  }
+  // status words of the last solves -> host (three ints: metric, Rayleigh-Ritz, its Cholesky factor)
+  void status_async(int* host) {
+    HALF_CUDA(cudaMemcpyAsync(host, info.get(), 3 * sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
   }
 };
 
@@ -255,7 +298,7 @@ struct Blocks {
 
 struct Scratch64 {
   DeviceBuffer<double2> metric, hsub, ssub;   // m x m, 2m x 2m, 2m x 2m
-  DeviceBuffer<double> w, mu, norms, kinetic;
+  DeviceBuffer<double> w, mu, norms, kinetic, dsc;
   DeviceBuffer<int> idx;
 };
 
@@ -327,7 +370,7 @@ struct AccRun {
       convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(tmp2m.get(), ssb, (long long)m * m);
       ++rt.prof.launches;
     }
-    ss.hegvd(hs, ssb, m, sc.w.get());
+    ss.hegvd(hs, ssb, m, sc.w.get(), m);
     to_r(hs, m, blk.Y.get(), m, m, m);
     int nx = blk.cur ^ 1;
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, blk.Y.get(), m, zero, blk.X[nx].get(), n);
@@ -343,11 +386,13 @@ struct AccRun {
     HALF_LAUNCH("residual norms");
     norms.resize(m);
     HALF_CUDA(cudaMemcpyAsync(norms.data(), sc.norms.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
-    HALF_CUDA(cudaMemcpyAsync(infos, ss.info.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
+    ss.status_async(infos);
     HALF_CUDA(cudaStreamSynchronize(rt.stream));
     mark("residual");
     if (infos[0] != 0) fail(kInternal, "ACC correction metric eigensolve failed (info " + std::to_string(infos[0]) + ")");
     if (infos[1] != 0) fail(kInternal, "ACC small generalized eigensolve failed (info " + std::to_string(infos[1]) + ")");
+    if (infos[2] != 0)
+      fail(kInternal, "ACC Rayleigh-Ritz overlap is not positive definite (Cholesky info " + std::to_string(infos[2]) + ")");
     double mx = 0;
     for (double v : norms) mx = std::max(mx, v);
     return mx;
@@ -382,9 +427,16 @@ struct AccRun {
       ++rt.prof.launches;
     }
     mark("metric_gemm");
+    const double* dsc = nullptr;
+    if (ss.own) {
+      metric_diag_kernel<<<ceil_div(m, 256), 256, 0, rt.stream>>>(metric, m, sc.dsc.get());
+      metric_scale_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.dsc.get());
+      rt.prof.launches += 2;
+      dsc = sc.dsc.get();
+    }
     ss.heevd(metric, m, sc.mu.get());
     mark("heevd");
-    scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14);
+    scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14, dsc);
     ++rt.prof.launches;
     to_r(metric, m, blk.small.get(), m, m, m);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.P.get(), n, blk.small.get(), m, zero, blk.PU.get(), n);
@@ -402,7 +454,7 @@ struct AccRun {
       project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.sx(), blk.SPU.get(), tmp2m.get(), ssb);
     }
     mark("rr_gemm");
-    ss.hegvd(hs, ssb, 2 * m, sc.w.get());
+    ss.hegvd(hs, ssb, 2 * m, sc.w.get(), m);
     mark("hegvd");
     to_r(hs, 2 * m, blk.Y.get(), 2 * m, 2 * m, m);
     const C* ytop = blk.Y.get();
@@ -436,6 +488,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   sc.ssub.resize(size_t(4) * m * m);
   sc.w.resize(2 * m);
   sc.mu.resize(m);
+  sc.dsc.resize(m);
   sc.norms.resize(m);
   sc.kinetic.upload(ks.basis.kinetic, rt.stream);
   auto order = kinetic_order(ks.basis.kinetic);
@@ -444,7 +497,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   SmallSolver ss(rt, m, sc.hsub.get(), sc.ssub.get(), sc.w.get());
   const double seed_threshold = std::max(cfg.tol * 1e-2, 1e-12);
   std::vector<double> norms;
-  int infos[2] = {0, 0};
+  int infos[3] = {0, 0, 0};
   int iter = 0, fp64_iter = 0;
   bool converged = false;
   double max_res = HUGE_VAL;

@@ -445,6 +445,7 @@ int half_solve_kpoint(half_handle handle, const double kpoint[3], int nbands, do
   if (nbands < 1) { export_error("band count must be positive", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
   return guarded(error, cap, [&]() -> int {
     SolveOutput out;
+    out.keep_device = vectors != nullptr;   // copied out below with the caller's leading dimension
     std::unique_ptr<KOperatorSet> ks;
     solve_one(*ctx, kpoint, nbands, false, out, &ks);
     long long n = ks->basis.npw();
@@ -708,6 +709,7 @@ extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoint
     std::vector<SolveOutput> outs(nk);
     std::vector<double> eig((size_t)nk * nbands);
     for (int ik = 0; ik < nk; ++ik) {
+      outs[ik].keep_device = true;   // the force needs the eigenvectors on the device
       solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik]);
       std::copy(outs[ik].eigenvalues.begin(), outs[ik].eigenvalues.end(), eig.begin() + (size_t)ik * nbands);
     }

@@ -8,6 +8,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -122,5 +124,24 @@ template <typename C> __host__ __device__ inline C cconjmul(C a, C b) {  // conj
 template <typename C, typename R> __host__ __device__ inline C cscale(C a, R s) { C r; r.x = a.x * s; r.y = a.y * s; return r; }
 
 inline int ceil_div(long long a, long long b) { return int((a + b - 1) / b); }
+
+// Raise, never lower, a kernel's dynamic shared-memory limit on the current
+// device.  The limit is a property of the function shared by every thread of
+// the process, so concurrent callers with different launch sizes (k points
+// whose sphere spans a different number of planes) must not shrink each
+// other's limit between the set and the launch.
+template <typename F>
+void raise_smem_limit(F* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limits;
+  if (bytes <= 48 * 1024) return;
+  int dev = 0;
+  HALF_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limits[{dev, reinterpret_cast<const void*>(kernel)}];
+  if (bytes <= cur) return;
+  HALF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+  cur = bytes;
+}
 
 }  // namespace hb

@@ -146,6 +146,7 @@ struct SolveOutput {
   std::vector<double> eigenvalues;
   std::vector<double> vectors;       // interleaved complex, npw x nbands (optional)
   double overlap_min = -1, overlap_max = -1;
+  bool keep_device = false;          // request dvectors even without host vectors
   DeviceBuffer<double2> dvectors;    // device copy (kept for forces)
 };
 void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out, SolveInfo& info);

@@ -152,10 +152,12 @@ void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, b
   auto* H = reinterpret_cast<cuDoubleComplex*>(h.get());
   auto* S = reinterpret_cast<cuDoubleComplex*>(s.get());
   int lwork = 0, hinfo = 0;
+  // eigenvectors are formed for the host copy or for a caller that keeps them on the device (forces)
+  const bool compute_vectors = want_vectors || out.keep_device;
   if (index_range) {
     // src/half_cuda_solver.cuf:119-144: only the lowest nbands, no overlap solve
     int meig = 0;
-    cusolverEigMode_t jobz = want_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+    cusolverEigMode_t jobz = compute_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
     cusolver_check(cusolverDnZhegvdx_bufferSize(rt.solver, CUSOLVER_EIG_TYPE_1, jobz, CUSOLVER_EIG_RANGE_I,
                                                 CUBLAS_FILL_MODE_UPPER, n, H, n, S, n, 0.0, 0.0, 1, nbands, &meig,
                                                 w.get(), &lwork),
@@ -178,7 +180,7 @@ void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, b
                                                w.get(), &lwork),
                    "zheevd buffer");
     int lwork2 = 0;
-    cusolverEigMode_t jobz = want_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+    cusolverEigMode_t jobz = compute_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
     cusolver_check(cusolverDnZhegvd_bufferSize(rt.solver, CUSOLVER_EIG_TYPE_1, jobz, CUBLAS_FILL_MODE_UPPER, n, H, n, S,
                                                n, w.get(), &lwork2),
                    "zhegvd buffer");
@@ -204,8 +206,13 @@ void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, b
   HALF_CUDA(cudaMemcpyAsync(ev.data(), w.get(), n * sizeof(double), cudaMemcpyDeviceToHost, st));
   HALF_CUDA(cudaStreamSynchronize(st));
   out.eigenvalues.assign(ev.begin(), ev.begin() + nbands);
-  out.dvectors.resize((size_t)n * nbands);
-  HALF_CUDA(cudaMemcpyAsync(out.dvectors.get(), h.get(), (size_t)n * nbands * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  if (compute_vectors) {
+    out.dvectors.resize((size_t)n * nbands);
+    HALF_CUDA(cudaMemcpyAsync(out.dvectors.get(), h.get(), (size_t)n * nbands * sizeof(double2),
+                              cudaMemcpyDeviceToDevice, st));
+  } else {
+    out.dvectors.release();
+  }
   if (want_vectors) {
     out.vectors.resize((size_t)2 * n * nbands);
     HALF_CUDA(cudaMemcpyAsync(out.vectors.data(), h.get(), (size_t)n * nbands * sizeof(double2), cudaMemcpyDeviceToHost, st));

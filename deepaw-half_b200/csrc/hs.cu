@@ -334,12 +334,9 @@ void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom
   op.col_qofs.upload(cq, s);
   HALF_LAUNCH("operator tables");
   HALF_CUDA(cudaStreamSynchronize(s));
-  HALF_CUDA(cudaFuncSetAttribute(k1_sphere_to_planes<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(plane_smem<R>(op.n2, op.n3))));
-  HALF_CUDA(cudaFuncSetAttribute(k3_planes_to_sphere<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(plane_smem<R>(op.n2, op.n3))));
-  HALF_CUDA(cudaFuncSetAttribute(k2_xlines<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(xline_smem<R>(op.n1, op.nplanes))));
+  raise_smem_limit(k1_sphere_to_planes<R>, plane_smem<R>(op.n2, op.n3));
+  raise_smem_limit(k3_planes_to_sphere<R>, plane_smem<R>(op.n2, op.n3));
+  raise_smem_limit(k2_xlines<R>, xline_smem<R>(op.n1, op.nplanes));
 }
 
 }  // namespace

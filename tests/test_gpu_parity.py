@@ -63,10 +63,16 @@ def test_evd_matches_dense_oracle(si2, oracle_system):
     from oracle import hamiltonian as H
     op = H.prepare(oracle_system("si2", si2))
     w, _, smin, smax = H.solve_dense(op, 16)
+    h, s = H.assemble_dense(op)
     with ctx_for(si2, solver="evd") as ctx:
         eg, _, gmin, gmax = ctx.solve((0, 0, 0), 16)
+        ev, vec, _, _ = ctx.solve((0, 0, 0), 16, vectors=True)
     assert np.abs(eg - w).max() <= 1e-10
     assert abs(gmin - smin) <= 1e-10 and abs(gmax - smax) <= 1e-10
+    assert np.array_equal(ev, eg)
+    # eigenpairs of the oracle's dense H, S with the zhegvd normalisation V^H S V = I
+    assert np.abs(h @ vec - (s @ vec) * ev[None, :]).max() <= 1e-9
+    assert np.abs(vec.conj().T @ s @ vec - np.eye(16)).max() <= 1e-10
 
 
 def test_index_range_solver(si2, oracle_system):
@@ -78,6 +84,9 @@ def test_index_range_solver(si2, oracle_system):
     assert np.abs(eg - w).max() <= 1e-10
     assert gmin == -1.0 and gmax == -1.0
     assert vec.shape == (op.basis.npw, 8)
+    h, s = H.assemble_dense(op)
+    assert np.abs(h @ vec - (s @ vec) * eg[None, :]).max() <= 1e-9
+    assert np.abs(vec.conj().T @ s @ vec - np.eye(8)).max() <= 1e-10
 
 
 def test_acc_fp64_iterates_match_oracle_acc(hfo2, oracle_system):
