@@ -660,6 +660,22 @@ int half_set_positions(half_handle handle, const double* positions, char* error,
   });
 }
 
+int half_set_positions_noalloc(half_handle handle, const double* positions, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (!positions) { export_error("positions pointer is required", error, cap); return HALF_ERROR_INVALID_ARGUMENT; }
+  return guarded(error, cap, [&]() -> int {
+    int n = ctx->crystal.nions();
+    for (int i = 0; i < 3 * n; ++i)
+      if (!std::isfinite(positions[i])) fail(kInvalidArgument, "positions must be finite");
+    ctx->rebuild_dij_fixed_scratch(true);   // capacity errors leave the context unchanged
+    ctx->crystal.positions.assign(positions, positions + 3 * n);
+    ctx->rebuild_dij_fixed_scratch(false);
+    return HALF_SUCCESS;
+  });
+}
+
 int half_nonlocal_forces(half_handle handle, const double kpoint[3], int nbands, int64_t ld, const HALF_C128* vectors,
                          const double* eigenvalues, const double* occupations, double kweight, double* forces,
                          char* error, int cap) {

@@ -112,6 +112,10 @@ struct Context {
 
   void initialize();                   // Veff + QDEP on the device
   void rebuild_dij();                  // QDEP at fixed Veff (positions changed)
+  // The same rebuild with every device scratch buffer in one fixed,
+  // statically allocated device array (no device allocation); check only
+  // reports whether this system fits it.
+  void rebuild_dij_fixed_scratch(bool check_only);
   long long nr() const { return (long long)charge.shape[0] * charge.shape[1] * charge.shape[2]; }
 };
 

@@ -11,6 +11,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
+#include <string>
 
 #include "context.h"
 
@@ -640,6 +642,176 @@ void Context::rebuild_dij() {
     sp.ddij.zero(rt->stream);
   }
   HALF_CUDA(cudaStreamSynchronize(rt->stream));
+}
+
+// ------------------------------------------------- fixed-scratch D_ij rebuild
+
+namespace {
+
+// Device scratch of the allocation-free rebuild (half_set_positions_noalloc):
+// a file-scope array, so the call needs no cudaMalloc/cudaFree.  It holds the
+// B-spline coefficients of Veff (8 B per grid point) followed by a region that
+// first holds the complex transform (16 B per point) and then, species by
+// species, the QDEP tables, the atom positions and the samples and radial
+// projections of a chunk of atoms.  Every word read is written earlier in the
+// same call, so nothing in it has to start at zero.  All calls on one device
+// share it: overlapping calls (any handle, any thread) race.
+constexpr size_t kFixedScratchBytes = size_t(32) << 20;
+constexpr int kMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
+
+std::mutex g_fixed_mutex;
+unsigned char* g_fixed_addr[kMaxDevices] = {};
+
+// Address of the scratch on the current device, resolved once per device.
+unsigned char* fixed_scratch() {
+  int dev = 0;
+  HALF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) fail(kInternal, "device ordinal out of range: " + std::to_string(dev));
+  std::lock_guard<std::mutex> lock(g_fixed_mutex);
+  if (!g_fixed_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_fixed_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      fail(kInternal, std::string("cudaGetSymbolAddress of the fixed D_ij scratch failed: ") + cudaGetErrorString(e));
+    }
+    g_fixed_addr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_fixed_addr[dev];
+}
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Bump allocator over a slice of the scratch; sizes were checked by the plan.
+struct Slice {
+  unsigned char* base;
+  size_t used = 0;
+  template <typename T>
+  T* take(size_t n) {
+    T* p = reinterpret_cast<T*>(base + used);
+    used += align256(n * sizeof(T));
+    return p;
+  }
+};
+
+// Atoms of one species that fit the region after its tables (0: not even one).
+int fixed_chunk(const SpeciesDevice& sp, size_t region) {
+  const QdepTables& t = sp.tables;
+  const size_t nang = t.dirs.size() / 3, ncomp = 4;
+  size_t fixed = align256(t.rgrid.size() * 8) + align256(t.dirs.size() * 8) + align256(t.yweight.size() * 8) +
+                 align256(t.wr2g.size() * 8) + align256(t.multipole.size() * 8) + align256(t.dion_lm.size() * 8) +
+                 align256(size_t(sp.natoms) * 3 * 8);
+  if (fixed + 2 * 256 >= region) return 0;
+  size_t per_atom = (size_t(t.nrad) * nang + t.naug) * ncomp * 8;
+  size_t fit = (region - fixed - 2 * 256) / per_atom;
+  return int(std::min<size_t>(fit, size_t(sp.natoms)));
+}
+
+}  // namespace
+
+void Context::rebuild_dij_fixed_scratch(bool check_only) {
+  cudaStream_t s = rt->stream;
+  if (!use_uspp) {   // DION only: copies into the existing D buffers
+    if (check_only) return;
+    for (auto& sp : species) {
+      const size_t per = sp.tables.dion_lm.size(), nd = size_t(sp.natoms) * per;
+      if (sp.dij.size() != nd || sp.ddij.size() != 3 * nd) fail(kInternal, "D_ij buffers were not set up");
+      sp.dij_host.resize(nd);
+      for (int a = 0; a < sp.natoms; ++a)
+        std::copy(sp.tables.dion_lm.begin(), sp.tables.dion_lm.end(), sp.dij_host.begin() + a * per);
+      HALF_CUDA(cudaMemcpyAsync(sp.dij.get(), sp.dij_host.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
+      sp.ddij.zero(s);
+    }
+    HALF_CUDA(cudaStreamSynchronize(s));
+    return;
+  }
+  const long long n = nr();
+  const size_t coeff_bytes = align256(size_t(n) * sizeof(double));
+  const size_t need_fft = coeff_bytes + align256(size_t(n) * sizeof(double2));
+  if (need_fft > kFixedScratchBytes)
+    fail(kCapacity, "the fixed D_ij scratch holds " + std::to_string(kFixedScratchBytes >> 20) + " MiB; a " +
+                        std::to_string(n) + "-point grid needs " + std::to_string(need_fft) +
+                        " bytes (24 B per point): use half_set_positions");
+  const size_t region = kFixedScratchBytes - coeff_bytes;
+  std::vector<int> chunk(species.size());
+  for (size_t it = 0; it < species.size(); ++it) {
+    chunk[it] = fixed_chunk(species[it], region);
+    if (chunk[it] < 1)
+      fail(kCapacity, "the QDEP tables of species " + std::to_string(it) + " do not fit the fixed " +
+                          std::to_string(kFixedScratchBytes >> 20) + " MiB D_ij scratch: use half_set_positions");
+    const SpeciesDevice& sp = species[it];
+    const size_t nd = size_t(sp.natoms) * sp.nlm * sp.nlm;
+    if (sp.dij.size() != nd || sp.ddij.size() != 3 * nd || sp.dij_host.size() != nd)
+      fail(kInternal, "D_ij buffers were not set up");
+  }
+  if (check_only) return;
+
+  unsigned char* base = fixed_scratch();
+  double* coeff = reinterpret_cast<double*>(base);
+  double2* freq = reinterpret_cast<double2*>(base + coeff_bytes);
+  const auto& sh = charge.shape;
+  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(veff.get(), freq, n, 1.0);
+  fft3d_inplace(freq, sh, -1, s);
+  prefilter_kernel<<<blocks_for(n), 256, 0, s>>>(freq, sh[0], sh[1], sh[2]);
+  fft3d_inplace(freq, sh, +1, s);
+  coeff_real_kernel<<<blocks_for(n), 256, 0, s>>>(freq, coeff, n);
+  HALF_LAUNCH("qdep prefilter");
+  SampleGeom geom{sh[0], sh[1], sh[2], {}};
+  auto inv = crystal.inverse_lattice();
+  for (int i = 0; i < 9; ++i) geom.inv[i] = inv[i];
+  const int ncomp = 4;
+  auto put = [&](double* dst, const std::vector<double>& v) {
+    HALF_CUDA(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  };
+  for (size_t it = 0; it < species.size(); ++it) {
+    SpeciesDevice& sp = species[it];
+    const QdepTables& t = sp.tables;
+    const int nang = int(t.dirs.size() / 3), na_max = chunk[it];
+    std::vector<double> pos;
+    for (int a = 0; a < sp.natoms; ++a) {
+      auto r = crystal.cartesian(sp.first_ion + a);
+      pos.insert(pos.end(), r.begin(), r.end());
+    }
+    // The region is reused: the copies below are ordered after every earlier
+    // kernel on this stream, including those still reading the transform.
+    Slice sl{base + coeff_bytes};
+    double* drg = sl.take<double>(t.rgrid.size());
+    double* ddirs = sl.take<double>(t.dirs.size());
+    double* dyw = sl.take<double>(t.yweight.size());
+    double* dwr = sl.take<double>(t.wr2g.size());
+    double* dmp = sl.take<double>(t.multipole.size());
+    double* ddion = sl.take<double>(t.dion_lm.size());
+    double* dpos = sl.take<double>(pos.size());
+    double* samples = sl.take<double>(size_t(na_max) * t.nrad * nang * ncomp);
+    double* radial = sl.take<double>(size_t(ncomp) * na_max * t.naug);
+    if (sl.used > region) fail(kInternal, "fixed D_ij scratch plan overflow");
+    put(drg, t.rgrid);
+    put(ddirs, t.dirs);
+    put(dyw, t.yweight);
+    put(dwr, t.wr2g);
+    put(dmp, t.multipole);
+    put(ddion, t.dion_lm);
+    put(dpos, pos);
+    const size_t nd = size_t(sp.nlm) * sp.nlm;
+    for (int a0 = 0; a0 < sp.natoms; a0 += na_max) {
+      const int na = std::min(na_max, sp.natoms - a0);
+      const long long total = (long long)na * t.nrad * nang;
+      sample_kernel<<<blocks_for(total), 256, 0, s>>>(coeff, dpos + 3 * a0, drg, ddirs, na, t.nrad, nang, geom, 1,
+                                                       samples);
+      HALF_LAUNCH("qdep sample");
+      project_radial_kernel<<<dim3(t.naug, na, ncomp), 256, 0, s>>>(samples, dyw, dwr, na, t.nrad, nang, t.naug,
+                                                                     ncomp, radial);
+      HALF_LAUNCH("qdep radial");
+      const long long npair = (long long)na * nd;
+      finish_dij_kernel<<<blocks_for(npair), 256, 0, s>>>(ddion, dmp, radial, na, sp.nlm, t.naug, ncomp,
+                                                           sp.dij.get() + a0 * nd, sp.ddij.get() + 3 * a0 * nd);
+      HALF_LAUNCH("qdep finish");
+    }
+    HALF_CUDA(cudaMemcpyAsync(sp.dij_host.data(), sp.dij.get(), sp.dij.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  }
+  HALF_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace hb

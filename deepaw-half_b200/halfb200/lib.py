@@ -83,6 +83,7 @@ _SIGS = {
     "half_get_last_solve_info": (C.c_int, [C.c_int64, _P] + _ERR),
     "half_solve_kpoints": (C.c_int, [C.c_int64, C.c_int, _P, C.c_int, _P] + _ERR),
     "half_set_positions": (C.c_int, [C.c_int64, _P] + _ERR),
+    "half_set_positions_noalloc": (C.c_int, [C.c_int64, _P] + _ERR),
     "half_nonlocal_forces": (C.c_int, [C.c_int64, _P, C.c_int, C.c_int64, _P, _P, _P, C.c_double, _P] + _ERR),
     "half_band_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P,
                                    _P] + _ERR),
@@ -267,6 +268,13 @@ class Context:
         err = self._err()
         p = np.ascontiguousarray(np.asarray(positions_fractional, dtype=np.float64).reshape(-1, 3))
         _check(self.lib.half_set_positions(self.handle, _ptr(p), err, 512), err)
+
+    def set_positions_noalloc(self, positions_fractional):
+        """``set_positions`` through the entry point that allocates no device
+        memory (fixed 32 MiB scratch; HALF_ERROR_CAPACITY beyond it)."""
+        err = self._err()
+        p = np.ascontiguousarray(np.asarray(positions_fractional, dtype=np.float64).reshape(-1, 3))
+        _check(self.lib.half_set_positions_noalloc(self.handle, _ptr(p), err, 512), err)
 
     def nonlocal_forces(self, k, vectors, eigenvalues, occupations, kweight):
         err = self._err()

@@ -76,6 +76,24 @@ int half_solve_kpoints(half_handle handle, int nk, const double *kpoints,
 int half_set_positions(half_handle handle, const double *positions_fractional,
                        char *error, int error_capacity);
 
+/* half_set_positions without device allocation (no counterpart in the
+ * reference).  For callers that must not allocate device memory in this call:
+ * a relaxation or MD driver that has reserved the rest of HBM for its own
+ * pool, or that keeps other streams busy and cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Results are identical to
+ * half_set_positions.
+ * Scratch: one fixed 32 MiB device array inside the library, shared by every
+ * handle on a device.  It must hold 24 bytes per grid point plus one atom's
+ * QDEP samples (about 1.5 MB); larger systems get HALF_ERROR_CAPACITY and
+ * the context is left unchanged.  Nothing in it needs to start at zero.
+ * Calls that overlap on one device (any handles, any threads) race on the
+ * scratch: serialise them.  The first call on each device resolves the
+ * scratch address (cudaGetSymbolAddress) and must not be made while a stream
+ * capture is in progress. */
+int half_set_positions_noalloc(half_handle handle,
+                               const double *positions_fractional,
+                               char *error, int error_capacity);
+
 /* Non-local PAW band-energy force for given eigenpairs at one k point
  * (src/half_forces.F90:9-73), accumulated into forces[nions*3] (atom-major,
  * eV/A).  vectors: npw x nbands, leading dimension ld >= npw; bands with zero
