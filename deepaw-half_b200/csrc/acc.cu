@@ -18,10 +18,11 @@
 //   cuBLAS/cuSOLVER handle lives on the context stream, and the only
 //   host<->device traffic per iteration is the m residual norms plus the
 //   solver status words (one synchronisation, as in the reference);
-// * with the library's own small eigensolver (eig.cu, HALF_SMALL_EIG=own) the
-//   correction metric is Jacobi-scaled before its eigendecomposition; the
-//   normalised directions span the same space, so the Ritz values are those
-//   of the reference up to rounding;
+// * with the library's own small solvers (eig.cu, the default) the
+//   correction directions are S-normalised by a Jacobi-scaled Cholesky
+//   factor (pivots floored at 1e-14) instead of the eigenvectors of the
+//   metric; both bases span the same space, so the Rayleigh-Ritz step and
+//   the Ritz values are those of the reference up to rounding;
 // * precision MIXED runs the iterations on FP32 blocks (FP32 operator,
 //   BF16x9 tensor-core GEMMs when cuBLAS provides them, FP64 small
 //   eigensolves) until the residual reaches the FP32 regime, then promotes X
@@ -32,6 +33,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <string>
 
 #include "blas.h"
 #include "context.h"
@@ -134,30 +136,11 @@ __global__ void precondition_kernel(const C* __restrict__ hx, const C* __restric
 }
 
 // U[:, j] /= sqrt(max(mu_j, floor))  (src/half_cuda_iterative_solver.cuf:66-77)
-// u[:, j] /= sqrt(max(mu_j, floor)); rows scaled by dsc[i] when the metric
-// was Jacobi-scaled (dsc == nullptr: no row scaling)
-__global__ void scale_columns_kernel(double2* u, int m, const double* mu, double floor_value, const double* dsc) {
+__global__ void scale_columns_kernel(double2* u, int m, const double* mu, double floor_value) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= m * m) return;
-  int j = t / m, i = t - j * m;
-  u[t] = cscale(u[t], (dsc ? dsc[i] : 1.0) / sqrt(fmax(mu[j], floor_value)));
-}
-
-// Jacobi scaling of the correction metric M = P^H S P for the library's own
-// small eigensolver: M <- D M D with D = diag(M)^-1/2.  P D U' spans what
-// P U spans, so the Rayleigh-Ritz step sees the same space; the spectrum of
-// D M D is O(1), whereas M itself carries one tiny eigenvalue per nearly
-// converged band (P columns of the size of their residuals), which the
-// bisection / inverse-iteration solver would treat as one large cluster.
-__global__ void metric_diag_kernel(const double2* __restrict__ M, int m, double* __restrict__ dsc) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < m) dsc[j] = 1.0 / sqrt(fmax(M[(size_t)j * m + j].x, DBL_MIN));
-}
-__global__ void metric_scale_kernel(double2* __restrict__ M, int m, const double* __restrict__ dsc) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= m * m) return;
-  int j = t / m, i = t - j * m;
-  M[t] = cscale(M[t], dsc[i] * dsc[j]);
+  int j = t / m;
+  u[t] = cscale(u[t], 1.0 / sqrt(fmax(mu[j], floor_value)));
 }
 
 template <typename A, typename B>
@@ -193,6 +176,12 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 // to stderr at the end of the solve.  Off by default (no synchronisation).
 struct Tracer {
   bool on = std::getenv("HALF_TRACE") != nullptr;
+  bool history = on && std::string(std::getenv("HALF_TRACE")) == "2";   // per-iteration residuals
+  void step(const char* phase, int it, double res, const std::vector<double>& norms) {
+    if (!history) return;
+    int worst = int(std::max_element(norms.begin(), norms.end()) - norms.begin());
+    std::fprintf(stderr, "HALF iter %s %d %.6e band %d\n", phase, it, res, worst);
+  }
   cudaStream_t s = nullptr;
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
   std::vector<std::pair<const char*, double>> acc;
@@ -215,8 +204,8 @@ struct Tracer {
 
 // FP64 small dense solves on the context's cuSOLVER handle; the status words
 // stay on the device and are read with the next residual norms.
-// By default cuSOLVER zheevd/zhegvd, as the reference does; environment
-// HALF_SMALL_EIG=own selects the library's device-resident solvers (eig.cu).
+// By default the library's own device-resident solvers (eig.cu); environment
+// HALF_SMALL_EIG=cusolver selects cuSOLVER zheevd/zhegvd as the reference does.
 struct SmallSolver {
   Runtime& rt;
   int m;
@@ -227,13 +216,10 @@ struct SmallSolver {
   SmallEigen eig;
   SmallSolver(Runtime& r, int m_, double2* a, double2* b, double* w) : rt(r), m(m_) {
     const char* sel = std::getenv("HALF_SMALL_EIG");
-    own = sel && std::string(sel) == "own";
+    own = !(sel && std::string(sel) == "cusolver");
     info.resize(3);
     info.zero(rt.stream);
-    if (own) {
-      eig.reserve(rt, 2 * m);
-      return;
-    }
+    if (own) eig.reserve(rt, 2 * m);
     int l1 = 0, l2 = 0, l3 = 0;
     cusolver_check(cusolverDnZheevd_bufferSize(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m,
                                                reinterpret_cast<cuDoubleComplex*>(a), m, w, &l1),
@@ -250,9 +236,9 @@ struct SmallSolver {
     lw_ev = l1;
     lw_gv = std::max(l2, l3);
   }
-  // all n eigenpairs of a (n x n)
+  // all n eigenpairs of a (n x n) (cuSOLVER in both modes: the metric of the
+  // own path goes through metric_normalize unless m is beyond its kernel)
   void heevd(double2* a, int n, double* w) {
-    if (own) { eig.heev(rt, a, n, n, w, info.get()); return; }
     cusolver_check(cusolverDnZheevd(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n,
                                     reinterpret_cast<cuDoubleComplex*>(a), n, w,
                                     reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()), info.get()),
@@ -298,7 +284,7 @@ struct Blocks {
 
 struct Scratch64 {
   DeviceBuffer<double2> metric, hsub, ssub;   // m x m, 2m x 2m, 2m x 2m
-  DeviceBuffer<double> w, mu, norms, kinetic, dsc;
+  DeviceBuffer<double> w, mu, norms, kinetic;
   DeviceBuffer<int> idx;
 };
 
@@ -427,17 +413,12 @@ struct AccRun {
       ++rt.prof.launches;
     }
     mark("metric_gemm");
-    const double* dsc = nullptr;
-    if (ss.own) {
-      metric_diag_kernel<<<ceil_div(m, 256), 256, 0, rt.stream>>>(metric, m, sc.dsc.get());
-      metric_scale_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.dsc.get());
-      rt.prof.launches += 2;
-      dsc = sc.dsc.get();
+    if (!(ss.own && ss.eig.metric_normalize(rt, metric, m, ss.info.get()))) {
+      ss.heevd(metric, m, sc.mu.get());
+      scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14);
+      ++rt.prof.launches;
     }
-    ss.heevd(metric, m, sc.mu.get());
     mark("heevd");
-    scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14, dsc);
-    ++rt.prof.launches;
     to_r(metric, m, blk.small.get(), m, m, m);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.P.get(), n, blk.small.get(), m, zero, blk.PU.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HP.get(), n, blk.small.get(), m, zero, blk.HPU.get(), n);
@@ -488,7 +469,6 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   sc.ssub.resize(size_t(4) * m * m);
   sc.w.resize(2 * m);
   sc.mu.resize(m);
-  sc.dsc.resize(m);
   sc.norms.resize(m);
   sc.kinetic.upload(ks.basis.kinetic, rt.stream);
   auto order = kinetic_order(ks.basis.kinetic);
@@ -529,6 +509,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     int since_best = 0;
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run32.residuals(norms, infos);
+      tracer.step("fp32", iter, max_res, norms);
       if (max_res < 0.9 * best) { best = max_res; since_best = 0; } else { ++since_best; }
       if (max_res <= switch_tol || since_best >= 6) break;
       run32.iterate(seed_threshold);
@@ -543,6 +524,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
       max_res = run64.residuals(norms, infos);
+      tracer.step("fp64", fp64_iter, max_res, norms);
       if (max_res <= cfg.tol) { converged = true; break; }
       run64.iterate(seed_threshold);
     }
@@ -555,6 +537,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run64.residuals(norms, infos);
+      tracer.step("fp64", iter, max_res, norms);
       if (max_res <= cfg.tol) { converged = true; break; }
       run64.iterate(seed_threshold);
     }

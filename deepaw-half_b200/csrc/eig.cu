@@ -35,6 +35,9 @@ namespace hb {
 namespace {
 
 constexpr int kEigThreads = 512;
+constexpr int kExtraEig = 8;   // eigenvalues located beyond the wanted ones (cluster at the cut)
+constexpr int kMetricMax = 164;   // packed triangle + two m-vectors within kSmemMax
+constexpr size_t kSmemMax = 226 * 1024;   // dynamic shared memory per CTA, leaving room for static
 
 // Number of eigenvalues of T below x (Sylvester inertia of T - x I).  The
 // pivots of the LDL^T factorisation are ratios q_i = p_i / p_{i-1} of the
@@ -69,54 +72,66 @@ __device__ int sturm_count(const double* d, const double* e2, int n, double x) {
 
 // LU factorisation with partial pivoting of T - lambda I (O(n)); the pivots
 // are stored inverted so that the solves multiply.  ai, b1, b2, l and piv are
-// per-thread scratch of length n.
+// per-thread scratch of n elements at stride st (the slots of a batch of
+// threads are interleaved, so a warp touches consecutive words).
 __device__ void tri_factor(const double* d, const double* e, int n, double lam, double tiny, double* ai, double* b1,
-                           double* b2, double* l, unsigned char* piv) {
+                           double* b2, double* l, unsigned char* piv, int st) {
   double diag = d[0] - lam, sup = n > 1 ? e[0] : 0.0;
   for (int i = 0; i < n - 1; ++i) {
     const double sub = e[i];
     const double nd = d[i + 1] - lam, ns = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+    const int o = i * st;
     if (fabs(diag) >= fabs(sub)) {
       if (fabs(diag) < tiny) diag = diag < 0 ? -tiny : tiny;
       const double r = 1.0 / diag, m = sub * r;
-      ai[i] = r; b1[i] = sup; b2[i] = 0.0; l[i] = m; piv[i] = 0;
+      ai[o] = r; b1[o] = sup; b2[o] = 0.0; l[o] = m; piv[o] = 0;
       diag = nd - m * sup;
       sup = ns;
     } else {
       const double r = 1.0 / sub, m = diag * r;
-      ai[i] = r; b1[i] = nd; b2[i] = ns; l[i] = m; piv[i] = 1;
+      ai[o] = r; b1[o] = nd; b2[o] = ns; l[o] = m; piv[o] = 1;
       diag = sup - m * nd;
       sup = -m * ns;
     }
   }
   if (fabs(diag) < tiny) diag = diag < 0 ? -tiny : tiny;
-  ai[n - 1] = 1.0 / diag;
-  b1[n - 1] = 0.0;
-  b2[n - 1] = 0.0;
+  const int o = (n - 1) * st;
+  ai[o] = 1.0 / diag;
+  b1[o] = 0.0;
+  b2[o] = 0.0;
 }
 
 __device__ void tri_solve(int n, const double* ai, const double* b1, const double* b2, const double* l,
-                          const unsigned char* piv, double* x) {
+                          const unsigned char* piv, double* x, int st) {
   for (int i = 0; i < n - 1; ++i) {
-    if (piv[i]) { double t = x[i]; x[i] = x[i + 1]; x[i + 1] = t - l[i] * x[i]; }
-    else x[i + 1] -= l[i] * x[i];
+    const int o = i * st;
+    if (piv[o]) { double t = x[o]; x[o] = x[o + st]; x[o + st] = t - l[o] * x[o]; }
+    else x[o + st] -= l[o] * x[o];
   }
-  x[n - 1] *= ai[n - 1];
-  if (n > 1) x[n - 2] = (x[n - 2] - b1[n - 2] * x[n - 1]) * ai[n - 2];
-  for (int i = n - 3; i >= 0; --i) x[i] = (x[i] - b1[i] * x[i + 1] - b2[i] * x[i + 2]) * ai[i];
+  x[(n - 1) * st] *= ai[(n - 1) * st];
+  if (n > 1) x[(n - 2) * st] = (x[(n - 2) * st] - b1[(n - 2) * st] * x[(n - 1) * st]) * ai[(n - 2) * st];
+  for (int i = n - 3; i >= 0; --i) {
+    const int o = i * st;
+    x[o] = (x[o] - b1[o] * x[o + st] - b2[o] * x[o + 2 * st]) * ai[o];
+  }
 }
 
 // One CTA: eigenvalues 0..nev-1 of T (ascending) and their eigenvectors Z (n x nev).
 __global__ void __launch_bounds__(kEigThreads) tridiag_eig_kernel(const double* __restrict__ d_in,
                                                                   const double* __restrict__ e_in, int n, int nev,
                                                                   double* __restrict__ w, double* __restrict__ Z,
-                                                                  double* __restrict__ scratch, int* __restrict__ status) {
+                                                                  double* __restrict__ gscratch, int batch,
+                                                                  int* __restrict__ status) {
+  // Eigenvalues up to ne = nev + kExtraEig are located so that a cluster
+  // straddling the last wanted index is computed (and orthogonalised) whole;
+  // only the first nev pairs are returned.
+  const int ne = min(n, nev + kExtraEig);
   extern __shared__ double sm[];
   double* d = sm;
   double* e = d + n;
   double* e2 = e + n;
   double* lam = e2 + n;
-  int* cl_first = reinterpret_cast<int*>(lam + nev);
+  int* cl_first = reinterpret_cast<int*>(lam + ne);
   __shared__ double s_gl, s_gu, s_norm;
   if (threadIdx.x == 0) *status = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -148,14 +163,14 @@ __global__ void __launch_bounds__(kEigThreads) tridiag_eig_kernel(const double* 
   // eps ||T|| (absolute accuracy eps ||T||, as bisection guarantees).
   {
     int g = 1;
-    while (g < 32 && 2 * g * nev <= int(blockDim.x)) g *= 2;
+    while (g < 32 && 2 * g * ne <= int(blockDim.x)) g *= 2;
     const int lane = threadIdx.x & 31, gl = lane & (g - 1), gbase = lane & ~(g - 1);
     const unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << gbase);
     const int groups = blockDim.x / g;
-    const int slots = (nev + groups - 1) / groups;   // same trip count on every thread
+    const int slots = (ne + groups - 1) / groups;   // same trip count on every thread
     for (int sidx = 0; sidx < slots; ++sidx) {
       const int k = sidx * groups + int(threadIdx.x) / g;
-      const bool active = k < nev;
+      const bool active = k < ne;
       double lo = s_gl, hi = s_gu;
       bool done = !active;
       for (int round = 0; round < 200; ++round) {
@@ -186,60 +201,80 @@ __global__ void __launch_bounds__(kEigThreads) tridiag_eig_kernel(const double* 
   const double ortol = 1.0e-7 * tnorm;
   if (threadIdx.x == 0) {
     int first = 0;
-    for (int k = 0; k < nev; ++k) {
+    for (int k = 0; k < ne; ++k) {
       if (k > 0 && lam[k] - lam[k - 1] > ortol) first = k;
       cl_first[k] = first;
     }
   }
   __syncthreads();
   for (int k = threadIdx.x; k < nev; k += blockDim.x) w[k] = lam[k];
-  // inverse iteration: the thread owning a cluster's first member computes the whole cluster
+  // Inverse iteration, in batches of `batch` threads whose scratch (five
+  // n-vectors and the pivot flags, interleaved by thread) sits in shared
+  // memory after the tables when it fits (gscratch == nullptr), else in
+  // global memory.  The thread owning a cluster's first member computes the
+  // whole cluster.
   const double tiny = DBL_EPSILON * tnorm;
-  double* ai = scratch + (size_t)threadIdx.x * 5 * n;
-  double* b1 = ai + n;
-  double* b2 = b1 + n;
-  double* l = b2 + n;
-  unsigned char* piv = reinterpret_cast<unsigned char*>(l + n);
-  for (int k0 = threadIdx.x; k0 < nev; k0 += blockDim.x) {
-    if (cl_first[k0] != k0) continue;
-    int k1 = k0;
-    while (k1 + 1 < nev && cl_first[k1 + 1] == k0) ++k1;
-    double prev = -HUGE_VAL;
-    for (int k = k0; k <= k1; ++k) {
-      double lk = lam[k];
-      // separate numerically equal eigenvalues of a cluster (dstein)
-      double sep = 10.0 * DBL_EPSILON * fmax(fabs(lk), tnorm * 1e-3);
-      if (k > k0 && lk - prev < sep) lk = prev + sep;
-      prev = lk;
-      tri_factor(d, e, n, lk, tiny, ai, b1, b2, l, piv);
-      double* x = Z + (size_t)k * n;
-      unsigned s = 0x9E3779B9u * (k + 1);
-      for (int i = 0; i < n; ++i) {   // deterministic pseudo-random start vector
-        s = s * 1664525u + 1013904223u;
-        x[i] = 1.0 + 0.5 * (double(s >> 8) / 16777216.0 - 0.5);
-      }
-      // three steps: with an eigenvalue accurate to rounding, each solve
-      // amplifies the wanted direction by ~1/eps
-      for (int it = 0; it < 3; ++it) {
-        tri_solve(n, ai, b1, b2, l, piv, x);
-        for (int j = k0; j < k; ++j) {   // Gram-Schmidt against earlier members of the cluster
-          const double* y = Z + (size_t)j * n;
-          double dot = 0;
-          for (int i = 0; i < n; ++i) dot += y[i] * x[i];
-          for (int i = 0; i < n; ++i) x[i] -= dot * y[i];
+  double* sbase = gscratch;
+  if (!sbase) {
+    size_t off = (3 * size_t(n) + ne) * sizeof(double) + size_t(ne) * sizeof(int);
+    off = (off + 15) & ~size_t(15);
+    sbase = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(sm) + off);
+  }
+  const int st = batch;
+  for (int b0 = 0; b0 < nev; b0 += batch) {
+    const int t = threadIdx.x;
+    const int k0 = b0 + t;
+    if (t < batch && k0 < nev && cl_first[k0] == k0) {
+      double* ai = sbase + t;
+      double* b1 = ai + size_t(n) * st;
+      double* b2 = b1 + size_t(n) * st;
+      double* l = b2 + size_t(n) * st;
+      double* x = l + size_t(n) * st;
+      unsigned char* piv = reinterpret_cast<unsigned char*>(sbase + 5 * size_t(n) * st) + t;
+      int k1 = k0;
+      while (k1 + 1 < ne && cl_first[k1 + 1] == k0) ++k1;
+      double prev = -HUGE_VAL;
+      for (int k = k0; k <= k1; ++k) {
+        double lk = lam[k];
+        // separate numerically equal eigenvalues of a cluster (dstein)
+        double sep = 10.0 * DBL_EPSILON * fmax(fabs(lk), tnorm * 1e-3);
+        if (k > k0 && lk - prev < sep) lk = prev + sep;
+        prev = lk;
+        tri_factor(d, e, n, lk, tiny, ai, b1, b2, l, piv, st);
+        unsigned s = 0x9E3779B9u * (k + 1);
+        for (int i = 0; i < n; ++i) {   // deterministic pseudo-random start vector
+          s = s * 1664525u + 1013904223u;
+          x[i * st] = 1.0 + 0.5 * (double(s >> 8) / 16777216.0 - 0.5);
         }
-        double nrm = 0;
-        for (int i = 0; i < n; ++i) nrm += x[i] * x[i];
-        nrm = sqrt(nrm);
-        if (!(nrm > 0) || !isfinite(nrm)) { atomicExch(status, 1); break; }
-        const double inv = 1.0 / nrm;
-        for (int i = 0; i < n; ++i) x[i] *= inv;
+        // With an eigenvalue accurate to rounding each solve amplifies the
+        // wanted direction by ~gap / (eps ||T||): two solves for an isolated
+        // eigenvalue, three (each followed by Gram-Schmidt against the earlier
+        // members) inside a cluster.
+        const int steps = k1 > k0 ? 3 : 2;
+        for (int it = 0; it < steps; ++it) {
+          tri_solve(n, ai, b1, b2, l, piv, x, st);
+          for (int j = k0; j < k; ++j) {
+            const double* y = Z + (size_t)j * n;
+            double dot = 0;
+            for (int i = 0; i < n; ++i) dot += y[i] * x[i * st];
+            for (int i = 0; i < n; ++i) x[i * st] -= dot * y[i];
+          }
+          double nrm = 0;
+          for (int i = 0; i < n; ++i) nrm += x[i * st] * x[i * st];
+          nrm = sqrt(nrm);
+          if (!(nrm > 0) || !isfinite(nrm)) { atomicExch(status, 1); break; }
+          const double inv = 1.0 / nrm;
+          for (int i = 0; i < n; ++i) x[i * st] *= inv;
+        }
+        // sign convention: largest component positive
+        double big = 0;
+        for (int i = 0; i < n; ++i) if (fabs(x[i * st]) > fabs(big)) big = x[i * st];
+        const double sg = big < 0 ? -1.0 : 1.0;
+        double* z = Z + (size_t)k * n;
+        for (int i = 0; i < n; ++i) z[i] = sg * x[i * st];
       }
-      // sign convention: largest component positive
-      double big = 0;
-      for (int i = 0; i < n; ++i) if (fabs(x[i]) > fabs(big)) big = x[i];
-      if (big < 0) for (int i = 0; i < n; ++i) x[i] = -x[i];
     }
+    __syncthreads();   // the next batch reuses the slots
   }
 }
 
@@ -293,6 +328,249 @@ __global__ void hermitian_fill_kernel(double2* A, int n) {
   }
 }
 
+// S-metric normalisation of the ACC correction block without an
+// eigendecomposition.  Given M = P^H S P (m x m, upper triangle read), write
+// U (m x m, upper triangular) with (P U)^H S (P U) = I up to the floor:
+//   D = diag(M)^-1/2,  D M D = R^H R (Cholesky, pivots floored at 1e-14),
+//   U = D R^-1.
+// P U spans what P spans (the reference's eigenvector basis U Lambda^-1/2
+// spans the same space), so the Rayleigh-Ritz step that follows sees the
+// same subspace; the floor plays the role of the reference's 1e-14 floor on
+// the metric eigenvalues for nearly dependent directions.  One CTA; the
+// packed upper triangle of D M D lives in shared memory (m <= kMetricMax).
+// *status = 1 if a pivot was not finite.
+__global__ void __launch_bounds__(512) metric_cholesky_kernel(double2* __restrict__ M, int m,
+                                                              int* __restrict__ status) {
+  extern __shared__ double2 pk[];   // packed upper: (i, j), i <= j at j (j + 1) / 2 + i
+  double* dsc = reinterpret_cast<double*>(pk + size_t(m) * (m + 1) / 2);
+  double2* col = reinterpret_cast<double2*>(dsc + m);
+  __shared__ double s_inv;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
+  if (tid == 0) s_bad = 0;
+  for (int j = tid; j < m; j += nt) dsc[j] = 1.0 / sqrt(fmax(M[size_t(j) * m + j].x, DBL_MIN));
+  __syncthreads();
+  for (int q = tid; q < m * m; q += nt) {
+    const int i = q % m, j = q / m;
+    if (i <= j) {
+      double2 v = M[size_t(j) * m + i];
+      if (i == j) v.y = 0.0;
+      pk[at(i, j)] = cscale(v, dsc[i] * dsc[j]);
+    }
+  }
+  __syncthreads();
+  // Right-looking Cholesky, row k of R overwrites row k of the triangle.  A
+  // pivot at or below 1e-14 (of the unit scaled diagonal) marks a direction
+  // dependent on the earlier ones to working precision: R(k,k) = 1e-7 and
+  // the rest of its row is zero, so the direction stays in the span without
+  // being eliminated from later columns (no growth from indefinite rounding).
+  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  for (int k = 0; k < m; ++k) {
+    if (tid == 0) {
+      double p = pk[at(k, k)].x;
+      if (!isfinite(p)) s_bad = 1;
+      double r = 1.0e-7, inv = 0.0;
+      if (p > 1.0e-14) { r = sqrt(p); inv = 1.0 / r; }
+      pk[at(k, k)] = make_double2(r, 0.0);
+      s_inv = inv;
+    }
+    __syncthreads();
+    const double inv = s_inv;
+    for (int j = k + 1 + tid; j < m; j += nt) {
+      const double2 v = cscale(pk[at(k, j)], inv);
+      pk[at(k, j)] = v;
+      col[j] = v;
+    }
+    __syncthreads();
+    if (inv != 0.0) {
+      for (int j = k + 1 + warp; j < m; j += nw) {   // A(i,j) -= conj(R(k,i)) R(k,j), k < i <= j
+        const double2 b = col[j];
+        double2* cj = pk + j * (j + 1) / 2;
+        for (int i = k + 1 + lane; i <= j; i += 32) {
+          const double2 a = col[i];
+          cj[i].x -= a.x * b.x + a.y * b.y;
+          cj[i].y -= a.x * b.y - a.y * b.x;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // X = R^-1 column by column, in place: X(i,j) = -X(i, i:j-1) R(i:j-1, j) / R(j,j)
+  for (int j = 0; j < m; ++j) {
+    for (int i = tid; i <= j; i += nt) col[i] = pk[at(i, j)];
+    __syncthreads();
+    const double rjj = col[j].x;
+    for (int i = warp; i < j; i += nw) {
+      double sr = 0, si = 0;
+      for (int k = i + lane; k < j; k += 32) {
+        const double2 x = pk[at(i, k)], r = col[k];
+        sr += x.x * r.x - x.y * r.y;
+        si += x.x * r.y + x.y * r.x;
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+      }
+      if (lane == 0) pk[at(i, j)] = make_double2(-sr / rjj, -si / rjj);
+    }
+    if (tid == 0) pk[at(j, j)] = make_double2(1.0 / rjj, 0.0);
+    __syncthreads();
+  }
+  // U = D X, lower triangle zero
+  for (int q = tid; q < m * m; q += nt) {
+    const int i = q % m, j = q / m;
+    M[q] = i <= j ? cscale(pk[at(i, j)], dsc[i]) : make_double2(0.0, 0.0);
+  }
+  if (tid == 0) *status = s_bad;
+}
+
+// Block-wide sum of a (real, imaginary) pair; every thread gets the result.
+__device__ double2 block_sum2(double a, double b, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, off);
+    b += __shfl_xor_sync(0xffffffffu, b, off);
+  }
+  __syncthreads();   // red may still be read by a previous call
+  if (lane == 0) { red[2 * warp] = a; red[2 * warp + 1] = b; }
+  __syncthreads();
+  double sa = 0, sb = 0;
+  for (int w = 0; w < nw; ++w) { sa += red[2 * w]; sb += red[2 * w + 1]; }
+  return make_double2(sa, sb);
+}
+
+// Householder reduction of a Hermitian A (n x n, upper triangle read) to the
+// real tridiagonal T = Q^H A Q, in the storage convention of LAPACK zhetrd
+// with UPLO = 'U' (the published zhetd2 algorithm): for i = n-2 .. 0 the
+// reflector H(i) = I - tau_i v v^H with v(i) = 1 and v(0:i-1) left in
+// A(0:i-1, i+1) annihilates A(0:i-1, i+1); d = diag(T), e = superdiagonal.
+// One CTA; the packed upper triangle stays in shared memory for the whole
+// reduction (n <= kMetricMax), replacing a launch pair per reflector.
+__global__ void __launch_bounds__(512) hetrd_kernel(double2* __restrict__ A, int n, double* __restrict__ dout,
+                                                    double* __restrict__ eout, double2* __restrict__ tauout) {
+  extern __shared__ double2 pk[];
+  double2* v = pk + size_t(n) * (n + 1) / 2;
+  double2* y = v + n;
+  __shared__ double red[64];
+  __shared__ double2 s_tau, s_scale, s_alpha2;
+  __shared__ double s_beta;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
+  for (int q = tid; q < n * n; q += nt) {
+    const int i = q % n, j = q / n;
+    if (i <= j) {
+      double2 a = A[q];
+      if (i == j) a.y = 0.0;
+      pk[at(i, j)] = a;
+    }
+  }
+  __syncthreads();
+  for (int i0 = n - 2; i0 >= 0; --i0) {
+    const int L = i0 + 1, c = i0 + 1;
+    // zlarfg on (alpha = A(i0, c), x = A(0:i0-1, c))
+    double part = 0;
+    for (int r = tid; r < i0; r += nt) {
+      const double2 x = pk[at(r, c)];
+      part += x.x * x.x + x.y * x.y;
+    }
+    const double xn2 = block_sum2(part, 0.0, red).x;
+    if (tid == 0) {
+      const double2 al = pk[at(i0, c)];
+      if (xn2 == 0.0 && al.y == 0.0) {
+        s_tau = make_double2(0.0, 0.0);
+        s_beta = al.x;
+        s_scale = make_double2(1.0, 0.0);
+      } else {
+        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
+        s_scale = make_double2(dr / den, -di / den);   // 1 / (alpha - beta)
+        s_beta = beta;
+      }
+    }
+    __syncthreads();
+    const double2 tau = s_tau, sc = s_scale;
+    for (int r = tid; r < L; r += nt) {
+      double2 vr = make_double2(1.0, 0.0);
+      if (r < i0) {
+        const double2 x = pk[at(r, c)];
+        vr = make_double2(x.x * sc.x - x.y * sc.y, x.x * sc.y + x.y * sc.x);
+        pk[at(r, c)] = vr;
+      }
+      v[r] = vr;
+    }
+    __syncthreads();
+    if (tau.x != 0.0 || tau.y != 0.0) {
+      // y = tau A(0:i0, 0:i0) v: g = 2^k threads per row, partial sums over
+      // s = p, p + g, ... combined by shuffles (deterministic order)
+      {
+        int lg = 0;
+        while (lg < 5 && (2 << lg) * L <= nt) ++lg;
+        const int g = 1 << lg, r = tid >> lg, p = tid & (g - 1);
+        double sr = 0, si = 0;
+        if (r < L) {
+          const double2* cr = pk + r * (r + 1) / 2;   // column r: A(s, r), s <= r
+          for (int s2 = p; s2 < L; s2 += g) {
+            double2 a;
+            if (r <= s2) a = pk[s2 * (s2 + 1) / 2 + r];
+            else { a = cr[s2]; a.y = -a.y; }
+            const double2 vv = v[s2];
+            sr += a.x * vv.x - a.y * vv.y;
+            si += a.x * vv.y + a.y * vv.x;
+          }
+        }
+        for (int off = g >> 1; off > 0; off >>= 1) {
+          sr += __shfl_xor_sync(0xffffffffu, sr, off);
+          si += __shfl_xor_sync(0xffffffffu, si, off);
+        }
+        if (r < L && p == 0) y[r] = make_double2(tau.x * sr - tau.y * si, tau.x * si + tau.y * sr);
+      }
+      __syncthreads();
+      // alpha2 = -tau (y^H v) / 2; w = y + alpha2 v
+      double pr = 0, pi = 0;
+      for (int r = tid; r < L; r += nt) {
+        const double2 yy = y[r], vv = v[r];
+        pr += yy.x * vv.x + yy.y * vv.y;   // conj(y) v
+        pi += yy.x * vv.y - yy.y * vv.x;
+      }
+      const double2 dot = block_sum2(pr, pi, red);
+      if (tid == 0) s_alpha2 = make_double2(-0.5 * (tau.x * dot.x - tau.y * dot.y), -0.5 * (tau.x * dot.y + tau.y * dot.x));
+      __syncthreads();
+      const double2 a2 = s_alpha2;
+      for (int r = tid; r < L; r += nt) {
+        const double2 vv = v[r];
+        y[r].x += a2.x * vv.x - a2.y * vv.y;
+        y[r].y += a2.x * vv.y + a2.y * vv.x;
+      }
+      __syncthreads();
+      // A(0:i0, 0:i0) -= v w^H + w v^H (upper triangle), one warp per column
+      for (int s2 = warp; s2 < L; s2 += nw) {
+        const double2 ws = y[s2], vs = v[s2];
+        double2* cs = pk + s2 * (s2 + 1) / 2;
+        for (int r = lane; r <= s2; r += 32) {
+          const double2 vr = v[r], wr = y[r];
+          cs[r].x -= (vr.x * ws.x + vr.y * ws.y) + (wr.x * vs.x + wr.y * vs.y);
+          cs[r].y -= (vr.y * ws.x - vr.x * ws.y) + (wr.y * vs.x - wr.x * vs.y);
+        }
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      eout[i0] = s_beta;
+      dout[i0 + 1] = pk[at(i0 + 1, i0 + 1)].x;
+      tauout[i0] = tau;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) dout[0] = pk[at(0, 0)].x;
+  for (int q = tid; q < n * n; q += nt) {   // reflector vectors back to A (strict upper triangle)
+    const int i = q % n, j = q / n;
+    if (i < j) A[q] = pk[at(i, j)];
+  }
+}
+
 }  // namespace
 
 void SmallEigen::reserve(Runtime& rt, int nmax) {
@@ -303,7 +581,7 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
   tau.resize(nmax);
   V.resize(size_t(nmax) * nmax);
   Z.resize(size_t(nmax) * nmax);
-  scratch.resize(size_t(kEigThreads) * 5 * nmax + 16);
+  scratch.resize(size_t(kEigThreads) * (5 * size_t(nmax) + (nmax + 7) / 8) + 16);
   info.resize(1);
   info.zero(rt.stream);
   int l1 = 0, l2 = 0;
@@ -322,14 +600,36 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
 void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* status) {
   reserve(rt, n);
   cudaStream_t s = rt.stream;
-  cusolver_check(cusolverDnZhetrd(rt.solver, CUBLAS_FILL_MODE_UPPER, n, reinterpret_cast<cuDoubleComplex*>(A), n,
-                                  d.get(), e.get(), reinterpret_cast<cuDoubleComplex*>(tau.get()),
-                                  reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()), info.get()),
-                 "zhetrd");
-  size_t sm = (3 * size_t(n) + nev) * sizeof(double) + size_t(nev) * sizeof(int);
-  if (sm > 227 * 1024 || size_t(n) * sizeof(double2) > 227 * 1024) fail(kCapacity, "subspace eigenproblem too large for the tridiagonal solver: n=" + std::to_string(n));
+  if (n <= kMetricMax) {   // whole reduction in one CTA
+    const size_t tsm = (size_t(n) * (n + 1) / 2 + 2 * size_t(n)) * sizeof(double2);
+    raise_smem_limit(hetrd_kernel, tsm);
+    hetrd_kernel<<<1, 512, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
+    HALF_LAUNCH("Householder tridiagonalisation");
+    rt.prof.launches += 1;
+  } else {
+    cusolver_check(cusolverDnZhetrd(rt.solver, CUBLAS_FILL_MODE_UPPER, n, reinterpret_cast<cuDoubleComplex*>(A), n,
+                                    d.get(), e.get(), reinterpret_cast<cuDoubleComplex*>(tau.get()),
+                                    reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()), info.get()),
+                   "zhetrd");
+  }
+  const int ne = std::min(n, nev + kExtraEig);
+  size_t sm = (3 * size_t(n) + ne) * sizeof(double) + size_t(ne) * sizeof(int);
+  if (sm > kSmemMax || size_t(n) * sizeof(double2) > kSmemMax)
+    fail(kCapacity, "subspace eigenproblem too large for the tridiagonal solver: n=" + std::to_string(n));
+  // inverse-iteration slots: in shared memory when at least 32 fit, else global
+  sm = (sm + 15) & ~size_t(15);
+  const size_t per_slot = 5 * size_t(n) * sizeof(double) + size_t(n);
+  int batch = int(std::min<size_t>((kSmemMax - sm) / per_slot, size_t(kEigThreads)));
+  batch = std::min(batch, (nev + 31) / 32 * 32) / 32 * 32;
+  double* gs = nullptr;
+  if (batch >= 32) {
+    sm += size_t(batch) * per_slot;
+  } else {
+    batch = kEigThreads;
+    gs = scratch.get();
+  }
   raise_smem_limit(tridiag_eig_kernel, sm);
-  tridiag_eig_kernel<<<1, kEigThreads, sm, s>>>(d.get(), e.get(), n, nev, w, Z.get(), scratch.get(), status);
+  tridiag_eig_kernel<<<1, kEigThreads, sm, s>>>(d.get(), e.get(), n, nev, w, Z.get(), gs, batch, status);
   HALF_LAUNCH("tridiagonal eigensolver");
   const int warps = n <= 384 ? 4 : 1;   // one n-vector of shared memory per warp
   raise_smem_limit(back_transform_kernel, size_t(warps) * n * sizeof(double2));
@@ -345,6 +645,22 @@ void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* s
 void SmallEigen::hegv(Runtime& rt, double2* A, double2* B, int n, int nev, double* w, int* status, int* chol_status) {
   reserve(rt, n);
   cudaStream_t s = rt.stream;
+  if (n <= kMetricMax) {
+    // B -> X = D R^-1 with X^H B X = I (metric_cholesky_kernel), C = X^H A X,
+    // C V = V Lambda, Y = X V: the same pencil reduction as zhegvd's
+    // Cholesky / two triangular solves, with the factor inverted in shared
+    // memory and the products done by three small GEMMs
+    metric_normalize(rt, B, n, chol_status);
+    hermitian_fill_kernel<<<ceil_div((long long)n * n, 256), 256, 0, s>>>(A, n);
+    rt.prof.launches += 1;
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, one, A, n, B, n, zero, V.get(), n);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, n, n, n, one, B, n, V.get(), n, zero, A, n);
+    heev(rt, A, n, nev, w, status);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, nev, n, one, B, n, A, n, zero, V.get(), n);
+    HALF_CUDA(cudaMemcpyAsync(A, V.get(), size_t(n) * nev * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    return;
+  }
   auto* Bc = reinterpret_cast<cuDoubleComplex*>(B);
   auto* Ac = reinterpret_cast<cuDoubleComplex*>(A);
   cusolver_check(cusolverDnZpotrf(rt.solver, CUBLAS_FILL_MODE_UPPER, n, Bc, n,
@@ -363,6 +679,18 @@ void SmallEigen::hegv(Runtime& rt, double2* A, double2* B, int n, int nev, doubl
   cublas_check(cublasZtrsm(rt.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, nev,
                            &one, Bc, n, Ac, n),
                "ztrsm");
+}
+
+// U with (P U)^H S (P U) = I from M = P^H S P, overwriting M (see
+// metric_cholesky_kernel); false when m is beyond the shared-memory kernel.
+bool SmallEigen::metric_normalize(Runtime& rt, double2* M, int m, int* status) {
+  if (m > kMetricMax) return false;
+  const size_t sm = (size_t(m) * (m + 1) / 2 + m) * sizeof(double2) + size_t(m) * sizeof(double);
+  raise_smem_limit(metric_cholesky_kernel, sm);
+  metric_cholesky_kernel<<<1, 512, sm, rt.stream>>>(M, m, status);
+  HALF_LAUNCH("metric Cholesky");
+  rt.prof.launches += 1;
+  return true;
 }
 
 }  // namespace hb

@@ -17,6 +17,9 @@ struct SmallEigen {
   // A y = lambda B y, B Hermitian positive definite; Y^H B Y = I.
   // *chol_status (device) is zpotrf's info (> 0: B not positive definite).
   void hegv(Runtime& rt, double2* A, double2* B, int n, int nev, double* w, int* status, int* chol_status);
+  // ACC correction metric: M = P^H S P (m x m) -> U, upper triangular, with
+  // (P U)^H S (P U) = I; returns false (nothing launched) when m is too large.
+  bool metric_normalize(Runtime& rt, double2* M, int m, int* status);
 };
 
 }  // namespace hb
