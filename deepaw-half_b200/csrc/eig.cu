@@ -425,6 +425,167 @@ __global__ void __launch_bounds__(512) metric_cholesky_kernel(double2* __restric
   if (tid == 0) *status = s_bad;
 }
 
+// The same normalisation as metric_cholesky_kernel, blocked by 32 columns
+// for m <= kBlockedMax (1024 threads): per block row K, one warp factors the
+// diagonal block (shuffles, no CTA barrier per column), one warp per column
+// solves the panel R_KK^H R_K,J = A_K,J, and the trailing Hermitian update
+// is one warp-reduced dot product of two packed column segments per element.
+// The inverse X = R^-1 is built the same way: diagonal blocks by one warp
+// each, then block column J from T_KJ = sum_L X_KL R_LJ and X_KJ = -T_KJ X_JJ.
+// Dependent pivots (<= 1e-14 of the unit scaled diagonal) get R(k,k) = 1e-7
+// and a zero row, exactly as in the unblocked kernel.
+constexpr int kBlockedMax = 128;
+
+__global__ void __launch_bounds__(1024) metric_cholesky_blocked_kernel(double2* __restrict__ M, int m,
+                                                                       int* __restrict__ status) {
+  extern __shared__ double2 pk[];   // packed upper triangle, (i, j) at j (j + 1) / 2 + i
+  double* dsc = reinterpret_cast<double*>(pk + size_t(m) * (m + 1) / 2);
+  double* ipiv = dsc + m;                                   // 1 / R(k,k), 0 for a dependent pivot
+  double2* tmp = reinterpret_cast<double2*>(ipiv + m);      // T blocks, [column c][row r], m x 32
+  __shared__ int s_bad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
+  if (tid == 0) s_bad = 0;
+  for (int j = tid; j < m; j += nt) dsc[j] = 1.0 / sqrt(fmax(M[size_t(j) * m + j].x, DBL_MIN));
+  __syncthreads();
+  for (int j = warp; j < m; j += nw) {
+    const double dj = dsc[j];
+    for (int i = lane; i <= j; i += 32) {
+      double2 v = M[size_t(j) * m + i];
+      if (i == j) v.y = 0.0;
+      pk[at(i, j)] = cscale(v, dsc[i] * dj);
+    }
+  }
+  __syncthreads();
+  const int nblk = (m + 31) / 32;
+  for (int K = 0; K < nblk; ++K) {
+    const int K0 = 32 * K, b = min(32, m - K0), E = K0 + b;
+    if (warp == 0) {   // diagonal block: unblocked Cholesky by one warp, lane = column
+      const int c = K0 + lane;
+      for (int k = 0; k < b; ++k) {
+        const int kk = K0 + k;
+        const double p = pk[at(kk, kk)].x;
+        __syncwarp();
+        double r = 1.0e-7, inv = 0.0;
+        if (p > 1.0e-14) { r = sqrt(p); inv = 1.0 / r; }
+        if (lane == 0) {
+          if (!isfinite(p)) s_bad = 1;
+          ipiv[kk] = inv;
+          pk[at(kk, kk)] = make_double2(r, 0.0);
+        }
+        if (lane > k && lane < b) pk[at(kk, c)] = cscale(pk[at(kk, c)], inv);
+        __syncwarp();
+        if (lane > k && lane < b && inv != 0.0) {
+          const double2 rc = pk[at(kk, c)];
+          for (int i = kk + 1; i <= c; ++i) {
+            const double2 a = pk[at(kk, i)];
+            double2& t = pk[at(i, c)];
+            t.x -= a.x * rc.x + a.y * rc.y;
+            t.y -= a.x * rc.y - a.y * rc.x;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // panel: R(K0:E, c) = R_KK^-H A(K0:E, c) for c >= E; lane = row, forward substitution
+    for (int c = E + warp; c < m; c += nw) {
+      double2 a = lane < b ? pk[at(K0 + lane, c)] : make_double2(0.0, 0.0);
+      for (int i = 0; i < b; ++i) {
+        const double xi_r = __shfl_sync(0xffffffffu, a.x, i) * ipiv[K0 + i];
+        const double xi_i = __shfl_sync(0xffffffffu, a.y, i) * ipiv[K0 + i];
+        if (lane == i) a = make_double2(xi_r, xi_i);
+        if (lane > i && lane < b) {
+          const double2 r = pk[at(K0 + i, K0 + lane)];   // R(i, lane): a -= conj(r) x_i
+          a.x -= r.x * xi_r + r.y * xi_i;
+          a.y -= r.x * xi_i - r.y * xi_r;
+        }
+      }
+      if (lane < b) pk[at(K0 + lane, c)] = a;
+    }
+    __syncthreads();
+    // trailing update: A(i,j) -= sum_l conj(R(K0+l, i)) R(K0+l, j), E <= i <= j
+    const int rem = m - E;
+    const int npair = rem * (rem + 1) / 2;
+    for (int q = warp; q < npair; q += nw) {
+      // q -> (i, j) with column-major packed order inside the trailing triangle
+      int j = int((sqrt(8.0 * q + 1.0) - 1.0) * 0.5);
+      while ((j + 1) * (j + 2) / 2 <= q) ++j;
+      while (j * (j + 1) / 2 > q) --j;
+      const int i = q - j * (j + 1) / 2;
+      const int gi = E + i, gj = E + j;
+      double sr = 0, si = 0;
+      if (lane < b) {
+        const double2 x = pk[at(K0 + lane, gi)], y = pk[at(K0 + lane, gj)];
+        sr = x.x * y.x + x.y * y.y;
+        si = x.x * y.y - x.y * y.x;
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, off);
+        si += __shfl_xor_sync(0xffffffffu, si, off);
+      }
+      if (lane == 0) {
+        pk[at(gi, gj)].x -= sr;
+        pk[at(gi, gj)].y -= si;
+      }
+    }
+    __syncthreads();
+  }
+  // inverse, diagonal blocks: warp K inverts R_KK in place (lane = row)
+  for (int K = warp; K < nblk; K += nw) {
+    const int K0 = 32 * K, b = min(32, m - K0);
+    for (int c = 0; c < b; ++c) {
+      const int gc = K0 + c;
+      const double rcc = pk[at(gc, gc)].x;   // R(c, c); column c is still R here
+      double sr = 0, si = 0;
+      if (lane < c) {   // X(lane, c) = -sum_{k=lane}^{c-1} X(lane, k) R(k, c) / R(c, c)
+        for (int k = lane; k < c; ++k) {
+          const double2 x = pk[at(K0 + lane, K0 + k)], r = pk[at(K0 + k, gc)];
+          sr += x.x * r.x - x.y * r.y;
+          si += x.x * r.y + x.y * r.x;
+        }
+      }
+      __syncwarp();
+      if (lane < c) pk[at(K0 + lane, gc)] = make_double2(-sr / rcc, -si / rcc);
+      if (lane == c) pk[at(gc, gc)] = make_double2(1.0 / rcc, 0.0);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // block columns J = 1 .. nblk-1: T_KJ = sum_{k = row}^{J0-1} X(row, k) R(k, c), rows < J0
+  for (int J = 1; J < nblk; ++J) {
+    const int J0 = 32 * J, bJ = min(32, m - J0);
+    for (int q = tid; q < J0 * bJ; q += nt) {
+      const int r = q % J0, c = q / J0;
+      double sr = 0, si = 0;
+      for (int k = r; k < J0; ++k) {
+        const double2 x = pk[at(r, k)], rr = pk[at(k, J0 + c)];
+        sr += x.x * rr.x - x.y * rr.y;
+        si += x.x * rr.y + x.y * rr.x;
+      }
+      tmp[c * J0 + r] = make_double2(sr, si);
+    }
+    __syncthreads();
+    for (int q = tid; q < J0 * bJ; q += nt) {   // X(r, J0+c) = -sum_{l<=c} T(r, l) X(J0+l, J0+c)
+      const int r = q % J0, c = q / J0;
+      double sr = 0, si = 0;
+      for (int l = 0; l <= c; ++l) {
+        const double2 t = tmp[l * J0 + r], x = pk[at(J0 + l, J0 + c)];
+        sr += t.x * x.x - t.y * x.y;
+        si += t.x * x.y + t.y * x.x;
+      }
+      pk[at(r, J0 + c)] = make_double2(-sr, -si);
+    }
+    __syncthreads();
+  }
+  for (int j = warp; j < m; j += nw) {   // U = D X, lower triangle zero
+    for (int i = lane; i < m; i += 32)
+      M[size_t(j) * m + i] = i <= j ? cscale(pk[at(i, j)], dsc[i]) : make_double2(0.0, 0.0);
+  }
+  if (tid == 0) *status = s_bad;
+}
+
 // Block-wide sum of a (real, imaginary) pair; every thread gets the result.
 __device__ double2 block_sum2(double a, double b, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -438,6 +599,146 @@ __device__ double2 block_sum2(double a, double b, double* red) {
   double sa = 0, sb = 0;
   for (int w = 0; w < nw; ++w) { sa += red[2 * w]; sb += red[2 * w + 1]; }
   return make_double2(sa, sb);
+}
+
+// hetrd_kernel for n <= kBlockedMax with 1024 threads: the product
+// u = A v reads each stored element once (warp w owns columns j = w mod 32,
+// lane owns rows i = lane + 32 t), A(i,j) v_j accumulates in registers and
+// conj(A(i,j)) v_i is warp-reduced into u_j; the per-warp row partials are
+// summed in a fixed order, so the result is deterministic.
+__global__ void __launch_bounds__(1024) hetrd_small_kernel(double2* __restrict__ A, int n, double* __restrict__ dout,
+                                                           double* __restrict__ eout, double2* __restrict__ tauout) {
+  extern __shared__ double2 pk[];
+  double2* v = pk + size_t(n) * (n + 1) / 2;
+  double2* y = v + n;
+  double2* yc = y + n;                 // column sums, one writer per column
+  double2* part = yc + n;              // [warp][row] register partials
+  __shared__ double red[64];
+  __shared__ double2 s_tau, s_scale, s_alpha2;
+  __shared__ double s_beta;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+  auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
+  for (int j = warp; j < n; j += nw)
+    for (int i = lane; i <= j; i += 32) {
+      double2 a = A[size_t(j) * n + i];
+      if (i == j) a.y = 0.0;
+      pk[at(i, j)] = a;
+    }
+  __syncthreads();
+  for (int i0 = n - 2; i0 >= 0; --i0) {
+    const int L = i0 + 1, c = i0 + 1;
+    double part2 = 0;
+    for (int r = tid; r < i0; r += nt) {
+      const double2 x = pk[at(r, c)];
+      part2 += x.x * x.x + x.y * x.y;
+    }
+    const double xn2 = block_sum2(part2, 0.0, red).x;
+    if (tid == 0) {
+      const double2 al = pk[at(i0, c)];
+      if (xn2 == 0.0 && al.y == 0.0) {
+        s_tau = make_double2(0.0, 0.0);
+        s_beta = al.x;
+        s_scale = make_double2(1.0, 0.0);
+      } else {
+        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
+        s_scale = make_double2(dr / den, -di / den);
+        s_beta = beta;
+      }
+    }
+    __syncthreads();
+    const double2 tau = s_tau, sc = s_scale;
+    for (int r = tid; r < L; r += nt) {
+      double2 vr = make_double2(1.0, 0.0);
+      if (r < i0) {
+        const double2 x = pk[at(r, c)];
+        vr = make_double2(x.x * sc.x - x.y * sc.y, x.x * sc.y + x.y * sc.x);
+        pk[at(r, c)] = vr;
+      }
+      v[r] = vr;
+    }
+    __syncthreads();
+    if (tau.x != 0.0 || tau.y != 0.0) {
+      double2 acc[4];
+      for (int t = 0; t < 4; ++t) acc[t] = make_double2(0.0, 0.0);
+      for (int j = warp; j < L; j += nw) {
+        const double2* cj = pk + j * (j + 1) / 2;
+        const double2 vj = v[j];
+        double tr = 0, ti = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int i = lane + 32 * t;
+          if (i <= j) {
+            const double2 a = cj[i];
+            acc[t].x += a.x * vj.x - a.y * vj.y;
+            acc[t].y += a.x * vj.y + a.y * vj.x;
+            if (i < j) {
+              const double2 vi = v[i];
+              tr += a.x * vi.x + a.y * vi.y;
+              ti += a.x * vi.y - a.y * vi.x;
+            }
+          }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+          tr += __shfl_xor_sync(0xffffffffu, tr, off);
+          ti += __shfl_xor_sync(0xffffffffu, ti, off);
+        }
+        if (lane == 0) yc[j] = make_double2(tr, ti);
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int i = lane + 32 * t;
+        if (i < L) part[warp * n + i] = acc[t];
+      }
+      __syncthreads();
+      for (int r = tid; r < L; r += nt) {   // y = tau (column sum + row partials in warp order)
+        double ur = yc[r].x, ui = yc[r].y;
+        for (int w = 0; w < nw; ++w) {
+          ur += part[w * n + r].x;
+          ui += part[w * n + r].y;
+        }
+        y[r] = make_double2(tau.x * ur - tau.y * ui, tau.x * ui + tau.y * ur);
+      }
+      __syncthreads();
+      double pr = 0, pi = 0;
+      for (int r = tid; r < L; r += nt) {
+        const double2 yy = y[r], vv = v[r];
+        pr += yy.x * vv.x + yy.y * vv.y;
+        pi += yy.x * vv.y - yy.y * vv.x;
+      }
+      const double2 dot = block_sum2(pr, pi, red);
+      if (tid == 0) s_alpha2 = make_double2(-0.5 * (tau.x * dot.x - tau.y * dot.y), -0.5 * (tau.x * dot.y + tau.y * dot.x));
+      __syncthreads();
+      const double2 a2 = s_alpha2;
+      for (int r = tid; r < L; r += nt) {
+        const double2 vv = v[r];
+        y[r].x += a2.x * vv.x - a2.y * vv.y;
+        y[r].y += a2.x * vv.y + a2.y * vv.x;
+      }
+      __syncthreads();
+      for (int s2 = warp; s2 < L; s2 += nw) {
+        const double2 ws = y[s2], vs = v[s2];
+        double2* cs = pk + s2 * (s2 + 1) / 2;
+        for (int r = lane; r <= s2; r += 32) {
+          const double2 vr = v[r], wr = y[r];
+          cs[r].x -= (vr.x * ws.x + vr.y * ws.y) + (wr.x * vs.x + wr.y * vs.y);
+          cs[r].y -= (vr.y * ws.x - vr.x * ws.y) + (wr.y * vs.x - wr.x * vs.y);
+        }
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      eout[i0] = s_beta;
+      dout[i0 + 1] = pk[at(i0 + 1, i0 + 1)].x;
+      tauout[i0] = tau;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) dout[0] = pk[at(0, 0)].x;
+  for (int j = warp; j < n; j += nw)
+    for (int i = lane; i < j; i += 32) A[size_t(j) * n + i] = pk[at(i, j)];
 }
 
 // Householder reduction of a Hermitian A (n x n, upper triangle read) to the
@@ -600,7 +901,13 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
 void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* status) {
   reserve(rt, n);
   cudaStream_t s = rt.stream;
-  if (n <= kMetricMax) {   // whole reduction in one CTA
+  if (n <= kBlockedMax) {   // whole reduction in one CTA, 1024 threads
+    const size_t tsm = (size_t(n) * (n + 1) / 2 + 3 * size_t(n) + 32 * size_t(n)) * sizeof(double2);
+    raise_smem_limit(hetrd_small_kernel, tsm);
+    hetrd_small_kernel<<<1, 1024, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
+    HALF_LAUNCH("Householder tridiagonalisation");
+    rt.prof.launches += 1;
+  } else if (n <= kMetricMax) {   // whole reduction in one CTA
     const size_t tsm = (size_t(n) * (n + 1) / 2 + 2 * size_t(n)) * sizeof(double2);
     raise_smem_limit(hetrd_kernel, tsm);
     hetrd_kernel<<<1, 512, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
@@ -685,6 +992,15 @@ void SmallEigen::hegv(Runtime& rt, double2* A, double2* B, int n, int nev, doubl
 // metric_cholesky_kernel); false when m is beyond the shared-memory kernel.
 bool SmallEigen::metric_normalize(Runtime& rt, double2* M, int m, int* status) {
   if (m > kMetricMax) return false;
+  if (m <= kBlockedMax) {
+    const size_t bsm = size_t(m) * (m + 1) / 2 * sizeof(double2) + 2 * size_t(m) * sizeof(double) +
+                       size_t(m) * 32 * sizeof(double2);
+    raise_smem_limit(metric_cholesky_blocked_kernel, bsm);
+    metric_cholesky_blocked_kernel<<<1, 1024, bsm, rt.stream>>>(M, m, status);
+    HALF_LAUNCH("metric Cholesky (blocked)");
+    rt.prof.launches += 1;
+    return true;
+  }
   const size_t sm = (size_t(m) * (m + 1) / 2 + m) * sizeof(double2) + size_t(m) * sizeof(double);
   raise_smem_limit(metric_cholesky_kernel, sm);
   metric_cholesky_kernel<<<1, 512, sm, rt.stream>>>(M, m, status);
