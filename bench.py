@@ -40,8 +40,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="hfo2")
-    p.add_argument("--tol", type=float, default=3e-5,
-                   help="ACC residual tolerance (eV); 3e-5 puts |d eps| below 1e-8 eV on this workload")
+    p.add_argument("--tol", type=float, default=2e-5,
+                   help="ACC residual tolerance (eV); 2e-5 keeps |d eps| below 1e-8 eV on this workload in both modes")
     p.add_argument("--max-iter", type=int, default=2000)
     p.add_argument("--block", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -187,7 +187,7 @@ def run_reference(args, rank, world):
     from halfb200 import synth
     w = synth.workload(args.workload)
     ch, po = write_inputs(w, rank)
-    iters = reference_iterations(args)
+    iters = reference_iterations(args) or args.max_iter
     base = CpuBaseline(w, ch, po)
     samples = []
     budget = max(2.0, 4 * args.cpu_sample_s / max(1, args.warmup + args.steps))
@@ -207,18 +207,20 @@ def run_reference(args, rank, world):
 
 
 # Iterations the reference acc algorithm (the oracle's FP64 restatement, LAPACK
-# small solves) needs to reach the bench tolerance 3e-5 eV on each workload,
-# from one complete oracle run to convergence (hfo2: 234 iterations, 228 s on
-# one host, max |d eps| = 5.8e-9 eV against the dense solve).  A complete run
-# is minutes of CPU time, so the reference arm times a bounded sample of
-# iterations and scales it by this count.
-REFERENCE_ITERATIONS = {"hfo2": 234}
+# small solves) needs to reach a residual tolerance on a workload, from
+# complete oracle runs to convergence on one host: hfo2 at 3e-5 eV, 234
+# iterations (228 s, max |d eps| = 5.8e-9 eV against the dense solve); at
+# 2e-5 eV, 267 iterations (267 s, 5.7e-9 eV).  A complete run is minutes of
+# CPU time, so the reference arm times a bounded sample of iterations and
+# scales it by this count.
+REFERENCE_ITERATIONS = {("hfo2", 3e-5): 234, ("hfo2", 2e-5): 267}
 
 
 def reference_iterations(args):
-    if args.workload in REFERENCE_ITERATIONS and abs(args.tol - 3e-5) < 1e-12:
-        return REFERENCE_ITERATIONS[args.workload]
-    return args.max_iter
+    for (name, tol), its in REFERENCE_ITERATIONS.items():
+        if name == args.workload and abs(args.tol - tol) < 1e-12:
+            return its
+    return None
 
 
 def main():
@@ -340,7 +342,10 @@ def main():
                                f"{w.nbands} bands, PBE, MIMIC_US D_ij", "tol_eV": args.tol,
                    "block": args.block, "kpoints_per_rank": nk, "l2": "flushed between steps (256 MB write)",
                    "parallelism": f"k-point ownership x{world}" if world > 1 else "single GPU"},
-        "max_abs_d_eps_eV": max(errs) if errs else None, "iterations": int(statistics.mean(i["iterations"] for i in infos)),
+        "max_abs_d_eps_eV": max(errs) if errs else None,
+        "per_step": [{"ms": round(t, 3), "iterations": i["iterations"], "fp64_iterations": i["fp64_iterations"]}
+                     for t, i in zip(dev_ms, infos)],
+        "iterations": int(statistics.mean(i["iterations"] for i in infos)),
         "fp64_refinement_iterations": int(statistics.mean(i["fp64_iterations"] for i in infos)),
         "wall_ms_per_step": statistics.mean(wall_ms),
         "fp64_mode": ({"ms_per_k": statistics.mean(fp64[0]) / nk_total, "iterations": fp64_iters,
@@ -361,7 +366,7 @@ def main():
                 "d2h_bytes_per_step": sum(8 * w.nbands + 16 * n * w.nbands for n in npw)},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ref_iters = REFERENCE_ITERATIONS.get(args.workload) if abs(args.tol - 3e-5) < 1e-12 else None
+        ref_iters = reference_iterations(args)
         line["cpu_baseline"] = cpu_baseline(w, ch, po, ref_iters or fp64_iters or line["iterations"],
                                             args.cpu_sample_s)
     if rank == 0:

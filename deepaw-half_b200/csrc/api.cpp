@@ -19,6 +19,7 @@
 
 #include "../../include/half_b200.h"
 #include "context.h"
+#include "devmem.h"
 
 using namespace hb;
 
@@ -150,6 +151,7 @@ void end_call(Runtime& rt, SolveInfo& info) {
   HALF_CUDA(cudaEventSynchronize(pf.b));
   float ms = 0;
   HALF_CUDA(cudaEventElapsedTime(&ms, pf.a, pf.b));
+  pf.collect();
   info.device_ms = ms;
   info.local_ms = pf.local_ms;
   info.local_bytes = pf.local_bytes;
@@ -274,6 +276,9 @@ int half_destroy(half_handle handle, char* error, int cap) {
   return guarded(error, cap, [&]() -> int {
     g_slots[s].ctx.reset();
     g_slots[s].used = false;
+    bool any = false;
+    for (const auto& sl : g_slots) any = any || sl.used;
+    if (!any) device_cache_release();   // last context gone: cached device blocks back to the driver
     return HALF_SUCCESS;
   });
 }

@@ -6,7 +6,9 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -49,7 +51,26 @@ inline void cusolver_check(cusolverStatus_t s, const char* what) {
 #define HALF_CUDA(x) ::hb::cuda_check((x), #x)
 #define HALF_LAUNCH(what) ::hb::cuda_check(cudaGetLastError(), what)
 
-// Owning device allocation.  Allocation failure is reported, never fatal.
+// With HALF_TRACE_ALLOC set, device allocations and frees slower than 5 ms are
+// reported (they synchronise the device and stall the host).
+struct AllocTimer {
+  const char* what;
+  size_t bytes;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  AllocTimer(const char* w, size_t b) : what(w), bytes(b) {}
+  ~AllocTimer() {
+    static const bool on = std::getenv("HALF_TRACE_ALLOC") != nullptr;
+    if (!on) return;
+    double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ms > 5.0) std::fprintf(stderr, "HALF slow %s: %.1f ms (%zu bytes)\n", what, ms, bytes);
+  }
+};
+
+void* device_alloc(size_t bytes, size_t* granted);   // devmem.cpp: caching allocator
+void device_free(void* p, size_t granted);
+
+// Owning device allocation through the caching allocator (devmem.h).
+// Allocation failure is reported, never fatal.
 template <typename T>
 class DeviceBuffer {
  public:
@@ -58,28 +79,25 @@ class DeviceBuffer {
   ~DeviceBuffer() { release(); }
   DeviceBuffer(const DeviceBuffer&) = delete;
   DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_), cap_(o.cap_) { o.p_ = nullptr; o.n_ = o.cap_ = 0; }
   DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
-    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+    if (this != &o) {
+      release();
+      p_ = o.p_; n_ = o.n_; cap_ = o.cap_;
+      o.p_ = nullptr; o.n_ = o.cap_ = 0;
+    }
     return *this;
   }
   void resize(size_t n) {
     if (n == n_) return;
     release();
-    if (n) {
-      cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p_), n * sizeof(T));
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        p_ = nullptr;
-        fail(kInternal, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " + cudaGetErrorString(e));
-      }
-    }
+    if (n) p_ = static_cast<T*>(device_alloc(n * sizeof(T), &cap_));
     n_ = n;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) device_free(p_, cap_);
     p_ = nullptr;
-    n_ = 0;
+    n_ = cap_ = 0;
   }
   T* get() const { return p_; }
   size_t size() const { return n_; }
@@ -102,7 +120,7 @@ class DeviceBuffer {
 
  private:
   T* p_ = nullptr;
-  size_t n_ = 0;
+  size_t n_ = 0, cap_ = 0;   // elements, granted bytes
 };
 
 // ---- complex helpers (double2 / float2) -----------------------------------

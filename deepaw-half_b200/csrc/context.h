@@ -38,14 +38,27 @@ struct SolveInfo {
 };
 
 // Event-based accounting of the library's own kernels.
+// Event-timed spans of one device call.  Spans are recorded without host
+// synchronisation; their durations are read once, when the call ends and its
+// stream has been synchronised (collect), so timing adds no bubbles.
 struct Profile {
-  cudaEvent_t a = nullptr, b = nullptr, la = nullptr, lb = nullptr, sa = nullptr, sb = nullptr;
+  enum Kind { kLocal = 0, kSweep = 1, kAdjoint = 2 };
+  cudaEvent_t a = nullptr, b = nullptr;
+  std::vector<cudaEvent_t> pool;                         // reused across calls
+  std::vector<std::pair<int, std::pair<int, int>>> spans;   // (kind, (begin, end) pool slots)
+  size_t used = 0;
   double local_ms = 0, local_bytes = 0, sweep_ms = 0, adjoint_ms = 0;
   long long local_columns = 0, launches = 0, sweep_columns = 0;
   void reset() {
     local_ms = local_bytes = sweep_ms = adjoint_ms = 0;
     local_columns = launches = sweep_columns = 0;
+    spans.clear();
+    used = 0;
   }
+  int record(cudaStream_t s);                // a pooled event recorded on s
+  void span(Kind k, int begin, int end) { spans.push_back({int(k), {begin, end}}); }
+  void collect();                            // after synchronisation: add the span durations
+  void destroy();
 };
 
 // Per-stream library handles.

@@ -140,7 +140,7 @@ void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec,
   docc.upload(occ, nb, st);
   DeviceBuffer<double2> w(size_t(4) * npw * nb), cc(size_t(4) * np * nb);
   Profile& pf = rt.prof;
-  HALF_CUDA(cudaEventRecord(pf.sa, st));
+  const int ev0 = pf.record(st);
   build_qpsi_kernel<<<ceil_div((long long)npw * nb, 256), 256, 0, st>>>(dvec, ld, npw, nb, ks.qvec.get(), w.get());
   HALF_LAUNCH("force qpsi");
   const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
@@ -148,11 +148,7 @@ void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec,
   force_epilogue_kernel<<<nions, 256, 0, st>>>(cc.get(), np, nb, datoms.get(), dd.get(), ddd.get(), dq.get(), deig.get(),
                                                docc.get(), kweight, dout.get());
   HALF_LAUNCH("force epilogue");
-  HALF_CUDA(cudaEventRecord(pf.sb, st));
-  HALF_CUDA(cudaEventSynchronize(pf.sb));
-  float ms = 0;
-  HALF_CUDA(cudaEventElapsedTime(&ms, pf.sa, pf.sb));
-  pf.adjoint_ms += ms;
+  pf.span(Profile::kAdjoint, ev0, pf.record(st));
   pf.launches += 2;
   auto f = dout.download(st);
   for (int i = 0; i < nions * 3; ++i) forces_host[i] += f[i];

@@ -442,8 +442,8 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
   const size_t psm = plane_smem<R>(op.n2, op.n3), xsm = xline_smem<R>(op.n1, op.nplanes);
   const int tiles = (op.n3 + kXTile - 1) / kXTile;
   Profile& pf = rt.prof;
-  HALF_CUDA(cudaEventRecord(pf.sa, s));
-  HALF_CUDA(cudaEventRecord(pf.la, s));
+  const int ev_sweep = pf.record(s);
+  const int ev_local = ev_sweep;
   for (int b0 = 0; b0 < nb; b0 += chunk) {
     int nbc = std::min(chunk, nb - b0);
     k1_sphere_to_planes<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
@@ -457,27 +457,19 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
     pf.launches += 3;
   }
   HALF_LAUNCH("local operator");
-  HALF_CUDA(cudaEventRecord(pf.lb, s));
+  pf.span(Profile::kLocal, ev_local, pf.record(s));
   {
     // FFT-path algorithmic bytes per band: read psi, write H psi and S psi, two
     // transforms x two passes x (read + write) of the box; Veff once per call.
     const double sz = sizeof(C), rz = sizeof(R), nr = double(op.n1) * op.n2 * op.n3;
     pf.local_bytes += nb * (3.0 * sz * op.npw + 8.0 * sz * nr) + rz * nr;
     pf.local_columns += nb;
-    HALF_CUDA(cudaEventSynchronize(pf.lb));
-    float ms = 0;
-    HALF_CUDA(cudaEventElapsedTime(&ms, pf.la, pf.lb));
-    pf.local_ms += ms;
   }
   if (op.np > 0) {
     pf.launches += 1;
     apply_nonlocal<R>(rt, op, x, ld, nb, hx, sx);
   }
-  HALF_CUDA(cudaEventRecord(pf.sb, s));
-  HALF_CUDA(cudaEventSynchronize(pf.sb));
-  float sms = 0;
-  HALF_CUDA(cudaEventElapsedTime(&sms, pf.sa, pf.sb));
-  pf.sweep_ms += sms;
+  pf.span(Profile::kSweep, ev_sweep, pf.record(s));
   pf.sweep_columns += nb;
 }
 

@@ -38,15 +38,41 @@ Runtime::Runtime() {
   if (bf16x9 && cublasSetMathMode(blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) != CUBLAS_STATUS_SUCCESS) bf16x9 = false;
   HALF_CUDA(cudaEventCreate(&prof.a));
   HALF_CUDA(cudaEventCreate(&prof.b));
-  HALF_CUDA(cudaEventCreate(&prof.la));
-  HALF_CUDA(cudaEventCreate(&prof.lb));
-  HALF_CUDA(cudaEventCreate(&prof.sa));
-  HALF_CUDA(cudaEventCreate(&prof.sb));
+}
+
+int Profile::record(cudaStream_t s) {
+  if (used == pool.size()) {
+    cudaEvent_t e = nullptr;
+    HALF_CUDA(cudaEventCreate(&e));
+    pool.push_back(e);
+  }
+  HALF_CUDA(cudaEventRecord(pool[used], s));
+  return int(used++);
+}
+
+void Profile::collect() {
+  for (const auto& sp : spans) {
+    float ms = 0;
+    HALF_CUDA(cudaEventElapsedTime(&ms, pool[sp.second.first], pool[sp.second.second]));
+    if (sp.first == kLocal) local_ms += ms;
+    else if (sp.first == kSweep) sweep_ms += ms;
+    else adjoint_ms += ms;
+  }
+  spans.clear();
+  used = 0;
+}
+
+void Profile::destroy() {
+  for (cudaEvent_t e : pool)
+    if (e) cudaEventDestroy(e);
+  pool.clear();
+  for (cudaEvent_t e : {a, b})
+    if (e) cudaEventDestroy(e);
+  a = b = nullptr;
 }
 
 Runtime::~Runtime() {
-  for (cudaEvent_t e : {prof.a, prof.b, prof.la, prof.lb, prof.sa, prof.sb})
-    if (e) cudaEventDestroy(e);
+  prof.destroy();
   if (solver) cusolverDnDestroy(solver);
   if (blas) cublasDestroy(blas);
   if (stream) cudaStreamDestroy(stream);
