@@ -601,146 +601,6 @@ __device__ double2 block_sum2(double a, double b, double* red) {
   return make_double2(sa, sb);
 }
 
-// hetrd_kernel for n <= kBlockedMax with 1024 threads: the product
-// u = A v reads each stored element once (warp w owns columns j = w mod 32,
-// lane owns rows i = lane + 32 t), A(i,j) v_j accumulates in registers and
-// conj(A(i,j)) v_i is warp-reduced into u_j; the per-warp row partials are
-// summed in a fixed order, so the result is deterministic.
-__global__ void __launch_bounds__(1024) hetrd_small_kernel(double2* __restrict__ A, int n, double* __restrict__ dout,
-                                                           double* __restrict__ eout, double2* __restrict__ tauout) {
-  extern __shared__ double2 pk[];
-  double2* v = pk + size_t(n) * (n + 1) / 2;
-  double2* y = v + n;
-  double2* yc = y + n;                 // column sums, one writer per column
-  double2* part = yc + n;              // [warp][row] register partials
-  __shared__ double red[64];
-  __shared__ double2 s_tau, s_scale, s_alpha2;
-  __shared__ double s_beta;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-  auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
-  for (int j = warp; j < n; j += nw)
-    for (int i = lane; i <= j; i += 32) {
-      double2 a = A[size_t(j) * n + i];
-      if (i == j) a.y = 0.0;
-      pk[at(i, j)] = a;
-    }
-  __syncthreads();
-  for (int i0 = n - 2; i0 >= 0; --i0) {
-    const int L = i0 + 1, c = i0 + 1;
-    double part2 = 0;
-    for (int r = tid; r < i0; r += nt) {
-      const double2 x = pk[at(r, c)];
-      part2 += x.x * x.x + x.y * x.y;
-    }
-    const double xn2 = block_sum2(part2, 0.0, red).x;
-    if (tid == 0) {
-      const double2 al = pk[at(i0, c)];
-      if (xn2 == 0.0 && al.y == 0.0) {
-        s_tau = make_double2(0.0, 0.0);
-        s_beta = al.x;
-        s_scale = make_double2(1.0, 0.0);
-      } else {
-        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
-        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
-        const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
-        s_scale = make_double2(dr / den, -di / den);
-        s_beta = beta;
-      }
-    }
-    __syncthreads();
-    const double2 tau = s_tau, sc = s_scale;
-    for (int r = tid; r < L; r += nt) {
-      double2 vr = make_double2(1.0, 0.0);
-      if (r < i0) {
-        const double2 x = pk[at(r, c)];
-        vr = make_double2(x.x * sc.x - x.y * sc.y, x.x * sc.y + x.y * sc.x);
-        pk[at(r, c)] = vr;
-      }
-      v[r] = vr;
-    }
-    __syncthreads();
-    if (tau.x != 0.0 || tau.y != 0.0) {
-      double2 acc[4];
-      for (int t = 0; t < 4; ++t) acc[t] = make_double2(0.0, 0.0);
-      for (int j = warp; j < L; j += nw) {
-        const double2* cj = pk + j * (j + 1) / 2;
-        const double2 vj = v[j];
-        double tr = 0, ti = 0;
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int i = lane + 32 * t;
-          if (i <= j) {
-            const double2 a = cj[i];
-            acc[t].x += a.x * vj.x - a.y * vj.y;
-            acc[t].y += a.x * vj.y + a.y * vj.x;
-            if (i < j) {
-              const double2 vi = v[i];
-              tr += a.x * vi.x + a.y * vi.y;
-              ti += a.x * vi.y - a.y * vi.x;
-            }
-          }
-        }
-        for (int off = 16; off > 0; off >>= 1) {
-          tr += __shfl_xor_sync(0xffffffffu, tr, off);
-          ti += __shfl_xor_sync(0xffffffffu, ti, off);
-        }
-        if (lane == 0) yc[j] = make_double2(tr, ti);
-      }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int i = lane + 32 * t;
-        if (i < L) part[warp * n + i] = acc[t];
-      }
-      __syncthreads();
-      for (int r = tid; r < L; r += nt) {   // y = tau (column sum + row partials in warp order)
-        double ur = yc[r].x, ui = yc[r].y;
-        for (int w = 0; w < nw; ++w) {
-          ur += part[w * n + r].x;
-          ui += part[w * n + r].y;
-        }
-        y[r] = make_double2(tau.x * ur - tau.y * ui, tau.x * ui + tau.y * ur);
-      }
-      __syncthreads();
-      double pr = 0, pi = 0;
-      for (int r = tid; r < L; r += nt) {
-        const double2 yy = y[r], vv = v[r];
-        pr += yy.x * vv.x + yy.y * vv.y;
-        pi += yy.x * vv.y - yy.y * vv.x;
-      }
-      const double2 dot = block_sum2(pr, pi, red);
-      if (tid == 0) s_alpha2 = make_double2(-0.5 * (tau.x * dot.x - tau.y * dot.y), -0.5 * (tau.x * dot.y + tau.y * dot.x));
-      __syncthreads();
-      const double2 a2 = s_alpha2;
-      for (int r = tid; r < L; r += nt) {
-        const double2 vv = v[r];
-        y[r].x += a2.x * vv.x - a2.y * vv.y;
-        y[r].y += a2.x * vv.y + a2.y * vv.x;
-      }
-      __syncthreads();
-      for (int s2 = warp; s2 < L; s2 += nw) {
-        const double2 ws = y[s2], vs = v[s2];
-        double2* cs = pk + s2 * (s2 + 1) / 2;
-        for (int r = lane; r <= s2; r += 32) {
-          const double2 vr = v[r], wr = y[r];
-          cs[r].x -= (vr.x * ws.x + vr.y * ws.y) + (wr.x * vs.x + wr.y * vs.y);
-          cs[r].y -= (vr.y * ws.x - vr.x * ws.y) + (wr.y * vs.x - wr.x * vs.y);
-        }
-      }
-      __syncthreads();
-    }
-    if (tid == 0) {
-      eout[i0] = s_beta;
-      dout[i0 + 1] = pk[at(i0 + 1, i0 + 1)].x;
-      tauout[i0] = tau;
-    }
-  }
-  __syncthreads();
-  if (tid == 0) dout[0] = pk[at(0, 0)].x;
-  for (int j = warp; j < n; j += nw)
-    for (int i = lane; i < j; i += 32) A[size_t(j) * n + i] = pk[at(i, j)];
-}
-
 // Householder reduction of a Hermitian A (n x n, upper triangle read) to the
 // real tridiagonal T = Q^H A Q, in the storage convention of LAPACK zhetrd
 // with UPLO = 'U' (the published zhetd2 algorithm): for i = n-2 .. 0 the
@@ -901,13 +761,7 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
 void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* status) {
   reserve(rt, n);
   cudaStream_t s = rt.stream;
-  if (n <= kBlockedMax) {   // whole reduction in one CTA, 1024 threads
-    const size_t tsm = (size_t(n) * (n + 1) / 2 + 3 * size_t(n) + 32 * size_t(n)) * sizeof(double2);
-    raise_smem_limit(hetrd_small_kernel, tsm);
-    hetrd_small_kernel<<<1, 1024, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
-    HALF_LAUNCH("Householder tridiagonalisation");
-    rt.prof.launches += 1;
-  } else if (n <= kMetricMax) {   // whole reduction in one CTA
+  if (n <= kMetricMax) {   // whole reduction in one CTA
     const size_t tsm = (size_t(n) * (n + 1) / 2 + 2 * size_t(n)) * sizeof(double2);
     raise_smem_limit(hetrd_kernel, tsm);
     hetrd_kernel<<<1, 512, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
