@@ -434,14 +434,14 @@ __global__ void __launch_bounds__(512) metric_cholesky_kernel(double2* __restric
 // each, then block column J from T_KJ = sum_L X_KL R_LJ and X_KJ = -T_KJ X_JJ.
 // Dependent pivots (<= 1e-14 of the unit scaled diagonal) get R(k,k) = 1e-7
 // and a zero row, exactly as in the unblocked kernel.
-constexpr int kBlockedMax = 128;
+constexpr int kBlockedMax = 144;   // packed triangle + T blocks ((m - 32) x 32) within kSmemMax
 
 __global__ void __launch_bounds__(1024) metric_cholesky_blocked_kernel(double2* __restrict__ M, int m,
                                                                        int* __restrict__ status) {
   extern __shared__ double2 pk[];   // packed upper triangle, (i, j) at j (j + 1) / 2 + i
   double* dsc = reinterpret_cast<double*>(pk + size_t(m) * (m + 1) / 2);
   double* ipiv = dsc + m;                                   // 1 / R(k,k), 0 for a dependent pivot
-  double2* tmp = reinterpret_cast<double2*>(ipiv + m);      // T blocks, [column c][row r], m x 32
+  double2* tmp = reinterpret_cast<double2*>(ipiv + m);      // T blocks, [column c][row r], (m - 32) x 32
   __shared__ int s_bad;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
@@ -848,7 +848,7 @@ bool SmallEigen::metric_normalize(Runtime& rt, double2* M, int m, int* status) {
   if (m > kMetricMax) return false;
   if (m <= kBlockedMax) {
     const size_t bsm = size_t(m) * (m + 1) / 2 * sizeof(double2) + 2 * size_t(m) * sizeof(double) +
-                       size_t(m) * 32 * sizeof(double2);
+                       size_t(std::max(m - 32, 1)) * 32 * sizeof(double2);
     raise_smem_limit(metric_cholesky_blocked_kernel, bsm);
     metric_cholesky_blocked_kernel<<<1, 1024, bsm, rt.stream>>>(M, m, status);
     HALF_LAUNCH("metric Cholesky (blocked)");
