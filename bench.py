@@ -288,9 +288,10 @@ def main():
         return dev_ms, wall_ms, infos, errs
 
     with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
-        fp64 = None
+        fp64 = fp64g = None
         if not args.no_fp64:
             fp64 = run_mode(ctx, "fp64", max(1, min(args.steps, 2)), 1)
+            fp64g = run_mode(ctx, "fp64_guarded", max(1, min(args.steps, 2)), 1)
         with Clocks(local) as clk:
             dev_ms, wall_ms, infos, errs = run_mode(ctx, "mixed", args.steps, args.warmup)
         clocks = clk.summary()
@@ -351,6 +352,10 @@ def main():
         "fp64_mode": ({"ms_per_k": statistics.mean(fp64[0]) / nk_total, "iterations": fp64_iters,
                        "max_abs_d_eps_eV": max(fp64[3]) if fp64[3] else None} if fp64 else None),
         "mixed_speedup_vs_fp64": (statistics.mean(fp64[0]) / ms_step) if fp64 else None,
+        "fp64_guarded_mode": ({"ms_per_k": statistics.mean(fp64g[0]) / nk_total,
+                               "iterations": int(statistics.mean(i["iterations"] for i in fp64g[2])),
+                               "max_abs_d_eps_eV": max(fp64g[3]) if fp64g[3] else None} if fp64g else None),
+        "mixed_speedup_vs_fp64_guarded": (statistics.mean(fp64g[0]) / ms_step) if fp64g else None,
         "force_adjoint_ms": statistics.mean(adj), "forward_sweep_ms": statistics.mean(sweep),
         "force_over_sweep": statistics.mean(adj) / statistics.mean(sweep),
         "roofline": {"kernel": "local operator (K1 sphere->planes, K2 x-lines*Veff, K3 planes->sphere), FP32",

@@ -465,13 +465,15 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   if (2 * mreq > n) fail(kInvalidArgument, "ACC solver requires NBANDS <= NPL/2");
   const AccControls& cfg = ctx.acc;
   const bool mixed = cfg.precision == kMixed;
-  // The mixed mode carries guard bands (m/8, at least 4, within NPL/2): a
-  // requested edge band nearly degenerate with the first unrequested one
-  // otherwise converges at the block method's edge rate, which after the
-  // FP32 phase took up to ten times the FP64 iteration count.  Convergence
-  // is decided on the requested bands only; FP64 mode is the reference
-  // algorithm unchanged (no guard bands).
-  const int guard = mixed ? std::min(std::max(4, mreq / 8), n / 2 - mreq) : 0;
+  // The mixed and guarded modes carry guard bands (m/8, at least 4, within
+  // NPL/2): a requested edge band nearly degenerate with the first
+  // unrequested one otherwise converges at the block method's edge rate
+  // (after the FP32 phase up to ten times the FP64 iteration count), and a
+  // degenerate level cut by the band count can leave the block converged on
+  // a higher level.  Convergence is decided on the requested bands only; the
+  // FP64 mode is the reference algorithm unchanged (no guard bands).
+  const bool guarded = mixed || cfg.precision == kFP64Guarded;
+  const int guard = guarded ? std::min(std::max(4, mreq / 8), n / 2 - mreq) : 0;
   const int m = mreq + guard;
   Scratch64 sc;
   sc.metric.resize(size_t(m) * m);

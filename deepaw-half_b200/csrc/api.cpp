@@ -542,7 +542,8 @@ int half_set_acc_controls(half_handle handle, double tol, int max_iterations, in
   Context* ctx = lookup(handle);
   if (!ctx) return bad_handle(error, cap);
   if (!(tol > 0) || !std::isfinite(tol) || max_iterations < 1 || block_size < 1 ||
-      (precision != HALF_PRECISION_FP64 && precision != HALF_PRECISION_MIXED)) {
+      (precision != HALF_PRECISION_FP64 && precision != HALF_PRECISION_MIXED &&
+       precision != HALF_PRECISION_FP64_GUARDED)) {
     export_error("invalid ACC solver controls", error, cap);
     return HALF_ERROR_INVALID_ARGUMENT;
   }

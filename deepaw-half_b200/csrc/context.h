@@ -13,7 +13,7 @@
 
 namespace hb {
 
-enum Precision : int { kFP64 = 0, kMixed = 1 };
+enum Precision : int { kFP64 = 0, kMixed = 1, kFP64Guarded = 2 };
 
 // ACC controls; the defaults are the reference's (src/half_cuda_iterative_solver.cuf:113-118).
 struct AccControls {

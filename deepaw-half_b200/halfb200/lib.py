@@ -22,7 +22,7 @@ HALF_ERROR_INTERNAL = 6
 XC = {"lda": 1, "pbe": 2}
 BACKEND = {"auto": 0, "cpu": 1, "cuda": 2}
 SOLVER = {"evd": 1, "evj": 2, "vasp": 3, "evx": 3, "acc": 4}
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "fp64_guarded": 2}
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None

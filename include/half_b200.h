@@ -16,9 +16,18 @@ extern "C" {
 #endif
 
 enum half_precision {
-  HALF_PRECISION_FP64 = 0,   /* every operator application and GEMM in FP64 */
-  HALF_PRECISION_MIXED = 1   /* FP32 operator / tensor-core GEMMs, FP64 refinement */
+  HALF_PRECISION_FP64 = 0,         /* the reference's iteration, every step in FP64 */
+  HALF_PRECISION_MIXED = 1,        /* FP32 operator / tensor-core GEMMs, FP64 refinement,
+                                      guard bands */
+  HALF_PRECISION_FP64_GUARDED = 2  /* FP64 throughout, with guard bands */
 };
+/* Guard bands: the block carries m/8 extra bands (at least 4, within NPL/2)
+ * and convergence is decided on the requested m.  Without them the block
+ * iteration converges on the last requested band at the rate set by its gap
+ * to the first unrequested one, and when the band count cuts a degenerate
+ * level it can converge to a higher level than the m-th eigenvalue (the
+ * residual test accepts any converged eigenpairs); the reference's iteration
+ * has the same property. */
 
 /* ACC controls.  The reference's solve_block_harris_cuda_full takes
  * tolerance / max_iterations / block_size (src/half_cuda_iterative_solver.cuf:

@@ -167,3 +167,39 @@ def test_nonlocal_forces_match_oracle(si2, oracle_system):
     with ctx_for(si2) as ctx:
         f = ctx.nonlocal_forces((0, 0, 0), v, w, occ, 0.7)
     assert np.abs(f - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+
+
+def test_guard_bands_find_a_degenerate_level_cut_by_the_band_count(si2, oracle_system):
+    """When the band count cuts a degenerate level, the reference iteration may
+    converge on a higher level (the residual test accepts any converged
+    eigenpairs); the guarded FP64 and the mixed modes carry guard bands and
+    must return the lowest m eigenvalues of the dense solve."""
+    from oracle import hamiltonian as H
+    op = H.prepare(oracle_system("si2", si2))
+    w, _, _, _ = H.solve_dense(op, 16)
+    cut = [m for m in range(4, 12) if abs(w[m] - w[m - 1]) < 1e-6]
+    assert cut, "the Si cell has degenerate levels at Gamma"
+    m = cut[0]
+    with ctx_for(si2) as ctx:
+        for precision, tol in (("fp64_guarded", 1e-10), ("mixed", 1e-8)):
+            ctx.set_acc(tol=1e-7, max_iterations=400, precision=precision)
+            eg, _, _, _ = ctx.solve((0, 0, 0), m)
+            assert ctx.info()["converged"] == 1
+            assert np.abs(eg - w[:m]).max() <= tol, (precision, m, eg - w[:m])
+
+
+def test_guarded_and_mixed_match_dense_on_the_64_atom_cell(inputs_dir):
+    """c2-size check (64-atom Si, 11k plane waves, 160 bands, k = (0, 0, 1/4)):
+    the 160th band is the first member of a 4-fold level, which the unguarded
+    iteration can miss; the guarded modes agree with the dense solve."""
+    from conftest import workload_files
+    w, ch, po = workload_files("si64", inputs_dir)
+    k = tuple(w.kpoints[1])
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="evd") as d:
+        ref = d.solve(k, w.nbands)[0]
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
+        for precision, tol in (("mixed", 1e-8), ("fp64_guarded", 1e-8)):
+            ctx.set_acc(tol=2e-5, max_iterations=400, precision=precision)
+            e = ctx.solve(k, w.nbands)[0]
+            assert ctx.info()["converged"] == 1
+            assert np.abs(e - ref).max() <= tol, (precision, np.abs(e - ref).max())
