@@ -101,18 +101,35 @@ __device__ void tri_factor(const double* d, const double* e, int n, double lam, 
   b2[o] = 0.0;
 }
 
+// The running values of both sweeps stay in registers, so the dependent
+// chain of a step is one or two FMAs, not a shared-memory round trip.
 __device__ void tri_solve(int n, const double* ai, const double* b1, const double* b2, const double* l,
                           const unsigned char* piv, double* x, int st) {
-  for (int i = 0; i < n - 1; ++i) {
+  double cur = x[0];
+  for (int i = 0; i < n - 1; ++i) {   // forward: L^-1 with the row swaps
     const int o = i * st;
-    if (piv[o]) { double t = x[o]; x[o] = x[o + st]; x[o + st] = t - l[o] * x[o]; }
-    else x[o + st] -= l[o] * x[o];
+    const double nxt = x[o + st], li = l[o];
+    if (piv[o]) {
+      x[o] = nxt;
+      cur = cur - li * nxt;
+    } else {
+      x[o] = cur;
+      cur = nxt - li * cur;
+    }
   }
-  x[(n - 1) * st] *= ai[(n - 1) * st];
-  if (n > 1) x[(n - 2) * st] = (x[(n - 2) * st] - b1[(n - 2) * st] * x[(n - 1) * st]) * ai[(n - 2) * st];
-  for (int i = n - 3; i >= 0; --i) {
+  const int on = (n - 1) * st;
+  double x1 = cur * ai[on];   // x(i+1)
+  x[on] = x1;
+  if (n == 1) return;
+  const int om = (n - 2) * st;
+  double x0 = (x[om] - b1[om] * x1) * ai[om];   // x(i)
+  x[om] = x0;
+  for (int i = n - 3; i >= 0; --i) {   // backward: U^-1
     const int o = i * st;
-    x[o] = (x[o] - b1[o] * x[o + st] - b2[o] * x[o + 2 * st]) * ai[o];
+    const double xi = (x[o] - b1[o] * x0 - b2[o] * x1) * ai[o];
+    x[o] = xi;
+    x1 = x0;
+    x0 = xi;
   }
 }
 
