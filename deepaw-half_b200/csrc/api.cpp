@@ -584,6 +584,83 @@ int half_get_last_solve_info(half_handle handle, half_solve_info_v1* info, char*
   return HALF_SUCCESS;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Solve nk independent k points, up to ctx.kpoint_workers of them at a time,
+// each worker on its own stream with its own cuBLAS/cuSOLVER handles (one k
+// point's host-side solver latency overlaps another's device work).  sink(ik,
+// out, rt) runs on the worker that solved k point ik, before its next solve;
+// device work it enqueues on rt.stream is complete when this returns.
+template <typename Sink>
+void solve_batch(Context& ctx, int nk, const double* kpoints, int nbands, bool keep_device, Sink sink) {
+  const int workers = std::max(1, std::min(nk, ctx.kpoint_workers));
+  while ((int)ctx.workers.size() < workers - 1) ctx.workers.push_back(std::make_unique<Runtime>());
+  std::vector<SolveInfo> infos(nk);
+  std::vector<std::string> errors(workers);
+  std::vector<int> codes(workers, 0);
+  HALF_CUDA(cudaDeviceSynchronize());
+  cudaEvent_t t0;
+  HALF_CUDA(cudaEventCreate(&t0));
+  HALF_CUDA(cudaEventRecord(t0, ctx.rt->stream));
+  std::vector<cudaEvent_t> ends(workers);
+  for (auto& e : ends) HALF_CUDA(cudaEventCreate(&e));
+  auto body = [&](int w) {
+    Runtime& rt = w == 0 ? *ctx.rt : *ctx.workers[w - 1];
+    try {
+      for (int ik = w; ik < nk; ik += workers) {
+        SolveOutput out;
+        out.keep_device = keep_device;
+        solve_one(ctx, rt, kpoints + 3 * ik, nbands, false, out, infos[ik]);
+        sink(ik, out, rt);
+      }
+    } catch (const Error& e) {
+      codes[w] = e.status;
+      errors[w] = e.what();
+    } catch (const std::exception& e) {
+      codes[w] = HALF_ERROR_INTERNAL;
+      errors[w] = e.what();
+    }
+    cudaEventRecord(ends[w], rt.stream);
+  };
+  if (workers == 1) {
+    body(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w) pool.emplace_back(body, w);
+    for (auto& t : pool) t.join();
+  }
+  float span = 0;
+  for (int w = 0; w < workers; ++w) {
+    HALF_CUDA(cudaEventSynchronize(ends[w]));
+    float ms = 0;
+    HALF_CUDA(cudaEventElapsedTime(&ms, t0, ends[w]));
+    span = std::max(span, ms);
+    cudaEventDestroy(ends[w]);
+  }
+  cudaEventDestroy(t0);
+  for (int w = 0; w < workers; ++w)
+    if (codes[w] != 0) fail(codes[w], errors[w]);
+  SolveInfo total;
+  for (int ik = 0; ik < nk; ++ik) accumulate(total, infos[ik], ik == 0);
+  total.device_ms = span;   // wall span on the device of the whole batch
+  ctx.last = total;
+}
+
+bool device_pointer(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+extern "C" {
+
 int half_solve_kpoints(half_handle handle, int nk, const double* kpoints, int nbands, double* eigenvalues, char* error,
                        int cap) {
   clear_error(error, cap);
@@ -594,59 +671,45 @@ int half_solve_kpoints(half_handle handle, int nk, const double* kpoints, int nb
     return HALF_ERROR_INVALID_ARGUMENT;
   }
   return guarded(error, cap, [&]() -> int {
-    // k points are independent: up to `workers` of them run concurrently, each
-    // on its own stream with its own cuBLAS/cuSOLVER handles, so one k point's
-    // host-side solver latency overlaps another's device work.
-    const int workers = std::max(1, std::min(nk, ctx->kpoint_workers));
-    while ((int)ctx->workers.size() < workers - 1) ctx->workers.push_back(std::make_unique<Runtime>());
-    std::vector<SolveInfo> infos(nk);
-    std::vector<std::string> errors(workers);
-    std::vector<int> codes(workers, 0);
-    HALF_CUDA(cudaDeviceSynchronize());
-    cudaEvent_t t0;
-    HALF_CUDA(cudaEventCreate(&t0));
-    HALF_CUDA(cudaEventRecord(t0, ctx->rt->stream));
-    std::vector<cudaEvent_t> ends(workers);
-    for (auto& e : ends) HALF_CUDA(cudaEventCreate(&e));
-    auto body = [&](int w) {
-      Runtime& rt = w == 0 ? *ctx->rt : *ctx->workers[w - 1];
-      try {
-        for (int ik = w; ik < nk; ik += workers) {
-          SolveOutput out;
-          solve_one(*ctx, rt, kpoints + 3 * ik, nbands, false, out, infos[ik]);
-          std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues + (size_t)ik * nbands);
-        }
-      } catch (const Error& e) {
-        codes[w] = e.status;
-        errors[w] = e.what();
-      } catch (const std::exception& e) {
-        codes[w] = HALF_ERROR_INTERNAL;
-        errors[w] = e.what();
+    solve_batch(*ctx, nk, kpoints, nbands, false, [&](int ik, SolveOutput& out, Runtime&) {
+      std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues + (size_t)ik * nbands);
+    });
+    return HALF_SUCCESS;
+  });
+}
+
+int half_solve_kpoints_device(half_handle handle, int nk, const double* kpoints, int nbands,
+                              double* eigenvalues_device, HALF_C128* vectors_device, int64_t ld, char* error,
+                              int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || nbands < 1 || !eigenvalues_device || (vectors_device && ld < 1)) {
+    export_error("invalid k-point batch arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    if (!device_pointer(eigenvalues_device) || (vectors_device && !device_pointer(vectors_device)))
+      fail(kInvalidArgument, "eigenvalue and eigenvector buffers must be device memory");
+    if (vectors_device)
+      for (int ik = 0; ik < nk; ++ik) {
+        if (!finite3(kpoints + 3 * ik)) fail(kInvalidArgument, "k point must be finite");
+        if (build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoints + 3 * ik).npw() > ld)
+          fail(kCapacity, "eigenvector leading dimension is smaller than a k point's basis");
       }
-      cudaEventRecord(ends[w], rt.stream);
-    };
-    if (workers == 1) {
-      body(0);
-    } else {
-      std::vector<std::thread> pool;
-      for (int w = 0; w < workers; ++w) pool.emplace_back(body, w);
-      for (auto& t : pool) t.join();
-    }
-    float span = 0;
-    for (int w = 0; w < workers; ++w) {
-      HALF_CUDA(cudaEventSynchronize(ends[w]));
-      float ms = 0;
-      HALF_CUDA(cudaEventElapsedTime(&ms, t0, ends[w]));
-      span = std::max(span, ms);
-      cudaEventDestroy(ends[w]);
-    }
-    cudaEventDestroy(t0);
-    for (int w = 0; w < workers; ++w)
-      if (codes[w] != 0) fail(codes[w], errors[w]);
-    SolveInfo total;
-    for (int ik = 0; ik < nk; ++ik) accumulate(total, infos[ik], ik == 0);
-    total.device_ms = span;   // wall span on the device of the whole batch
-    ctx->last = total;
+    double2* vec = reinterpret_cast<double2*>(vectors_device);
+    solve_batch(*ctx, nk, kpoints, nbands, vectors_device != nullptr, [&](int ik, SolveOutput& out, Runtime& rt) {
+      HALF_CUDA(cudaMemcpyAsync(eigenvalues_device + (size_t)ik * nbands, out.eigenvalues.data(),
+                                size_t(nbands) * sizeof(double), cudaMemcpyHostToDevice, rt.stream));
+      if (!vec) return;
+      const size_t npw = out.dvectors.size() / size_t(nbands);
+      double2* dst = vec + (size_t)ik * ld * nbands;
+      HALF_CUDA(cudaMemcpy2DAsync(dst, ld * sizeof(double2), out.dvectors.get(), npw * sizeof(double2),
+                                  npw * sizeof(double2), nbands, cudaMemcpyDeviceToDevice, rt.stream));
+      if ((size_t)ld > npw)
+        HALF_CUDA(cudaMemset2DAsync(dst + npw, ld * sizeof(double2), 0, (ld - npw) * sizeof(double2), nbands,
+                                    rt.stream));
+    });
     return HALF_SUCCESS;
   });
 }

@@ -82,6 +82,8 @@ _SIGS = {
     "half_set_acc_controls": (C.c_int, [C.c_int64, C.c_double, C.c_int, C.c_int, C.c_int] + _ERR),
     "half_get_last_solve_info": (C.c_int, [C.c_int64, _P] + _ERR),
     "half_solve_kpoints": (C.c_int, [C.c_int64, C.c_int, _P, C.c_int, _P] + _ERR),
+    "half_solve_kpoints_device": (C.c_int, [C.c_int64, C.c_int, _P, C.c_int, C.c_void_p, C.c_void_p, C.c_int64]
+                                  + _ERR),
     "half_set_positions": (C.c_int, [C.c_int64, _P] + _ERR),
     "half_set_positions_noalloc": (C.c_int, [C.c_int64, _P] + _ERR),
     "half_nonlocal_forces": (C.c_int, [C.c_int64, _P, C.c_int, C.c_int64, _P, _P, _P, C.c_double, _P] + _ERR),
@@ -263,6 +265,17 @@ class Context:
         eig = np.zeros((len(ks), nbands))
         _check(self.lib.half_solve_kpoints(self.handle, len(ks), _ptr(ks), nbands, _ptr(eig), err, 512), err)
         return eig
+
+    def solve_kpoints_device(self, kpoints, nbands, eigenvalues_ptr, vectors_ptr=None, ld=0):
+        """half_solve_kpoints_device: eigenvalues (nk x nbands, float64) and
+        optionally eigenvectors (nk blocks of ld x nbands, complex128,
+        column-major) written to device memory at the given addresses (for
+        example ``tensor.data_ptr()`` of CUDA tensors)."""
+        err = self._err()
+        ks = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        _check(self.lib.half_solve_kpoints_device(self.handle, len(ks), _ptr(ks), nbands, C.c_void_p(eigenvalues_ptr),
+                                                  C.c_void_p(vectors_ptr) if vectors_ptr else None, ld, err, 512),
+               err)
 
     def set_positions(self, positions_fractional):
         err = self._err()

@@ -77,6 +77,21 @@ int half_solve_kpoints(half_handle handle, int nk, const double *kpoints,
                        int nbands, double *eigenvalues_eV,
                        char *error, int error_capacity);
 
+/* Batched solve with device-resident outputs: the additive "batched multi-k
+ * solve on device pointers" for callers that keep the eigenpairs on the GPU
+ * (no counterpart in ABI v1).  eigenvalues_device: device memory, nk x nbands
+ * (row-major [ik][band]).  vectors_device: device memory or NULL (values
+ * only); k point ik's eigenvectors are the column-major block at
+ * vectors_device + ik * ld * nbands, npw_k rows used and rows npw_k .. ld-1
+ * zeroed.  ld must be at least every k point's basis size, else
+ * HALF_ERROR_CAPACITY; host pointers give HALF_ERROR_INVALID_ARGUMENT.  The
+ * buffers are complete when the call returns.  Same per-k algorithm and
+ * concurrency as half_solve_kpoints. */
+int half_solve_kpoints_device(half_handle handle, int nk, const double *kpoints,
+                              int nbands, double *eigenvalues_device,
+                              HALF_C128 *vectors_device, int64_t ld,
+                              char *error, int error_capacity);
+
 /* Move the atoms at fixed Veff (positions fractional, atom-major, in the
  * context's type-major order).  Rebuilds the MIMIC_US D_ij and dD_ij/dR
  * (src/half_uspp.F90:137-241) and, at the next solve, the projector phases
