@@ -489,8 +489,9 @@ int half_solve_kpoint_mapped(half_handle handle, const double kpoint[3], int nba
   }
   return guarded(error, cap, [&]() -> int {
     SolveOutput out;
+    out.keep_device = true;   // the permutation runs on the device
     std::unique_ptr<KOperatorSet> ks;
-    solve_one(*ctx, kpoint, nbands, true, out, &ks);
+    solve_one(*ctx, kpoint, nbands, false, out, &ks);
     const Basis& b = ks->basis;
     long long n = b.npw();
     if (host_npw != n) fail(kInvalidArgument, "host and HALF plane-wave bases have different sizes");
@@ -508,7 +509,7 @@ int half_solve_kpoint_mapped(half_handle handle, const double kpoint[3], int nba
       }
       table[p] = int(hi);
     }
-    std::vector<long long> perm(n);
+    std::vector<int> src_row(n);   // host row perm[i] takes HALF row i
     for (long long i = 0; i < n; ++i) {
       int p = g_hash(b.gvec[3 * i], b.gvec[3 * i + 1], b.gvec[3 * i + 2], table_size), hit = -1;
       while (table[p] >= 0) {
@@ -518,15 +519,9 @@ int half_solve_kpoint_mapped(half_handle handle, const double kpoint[3], int nba
         p = (p + 1) % table_size;
       }
       if (hit < 0) fail(kInvalidArgument, "host and HALF plane-wave bases contain different G vectors");
-      perm[i] = hit;
+      src_row[hit] = int(i);
     }
-    double* dst = reinterpret_cast<double*>(vectors);
-    std::fill(dst, dst + 2 * ld * nbands, 0.0);
-    for (int bnd = 0; bnd < nbands; ++bnd)
-      for (long long i = 0; i < n; ++i) {
-        dst[2 * (bnd * ld + perm[i])] = out.vectors[2 * (bnd * n + i)];
-        dst[2 * (bnd * ld + perm[i]) + 1] = out.vectors[2 * (bnd * n + i) + 1];
-      }
+    gather_rows_to_host(*ctx->rt, out.dvectors.get(), n, nbands, src_row, ld, reinterpret_cast<double2*>(vectors));
     if (eigenvalues) std::copy(out.eigenvalues.begin(), out.eigenvalues.end(), eigenvalues);
     if (overlap_min) *overlap_min = out.overlap_min;
     if (overlap_max) *overlap_max = out.overlap_max;

@@ -170,6 +170,12 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
 void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, bool want_vectors, SolveOutput& out);
 void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s);   // device N x N
 
+// ----------------------------------------------------------------- mapped hand-off
+// host_dst (ld x nb, column-major) = rows of src (n x nb) in the order src_row
+// (host row j takes HALF row src_row[j]); rows n..ld-1 zero.  mapped.cu.
+void gather_rows_to_host(Runtime& rt, const double2* src, long long n, int nb, const std::vector<int>& src_row,
+                         long long ld, double2* host_dst);
+
 // ----------------------------------------------------------------- forces
 void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec, long long ld, int nb,
                             const double* eig, const double* occ, double kweight, double* forces_host);
