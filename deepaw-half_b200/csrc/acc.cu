@@ -220,7 +220,7 @@ struct SmallSolver {
     own = !(sel && std::string(sel) == "cusolver");
     info.resize(3);
     info.zero(rt.stream);
-    if (own) eig.reserve(rt, 2 * m);
+    if (own && 2 * m <= SmallEigen::kOwnMaxOrder) eig.reserve(rt, 2 * m);
     int l1 = 0, l2 = 0, l3 = 0;
     cusolver_check(cusolverDnZheevd_bufferSize(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m,
                                                reinterpret_cast<cuDoubleComplex*>(a), m, w, &l1),
@@ -247,7 +247,7 @@ struct SmallSolver {
   }
   // generalized problem of order n; the nev lowest eigenvectors are wanted
   void hegvd(double2* a, double2* b, int n, double* w, int nev) {
-    if (own) { eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2); return; }
+    if (own && n <= SmallEigen::kOwnMaxOrder) { eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2); return; }
     cusolver_check(cusolverDnZhegvd(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
                                     n, reinterpret_cast<cuDoubleComplex*>(a), n, reinterpret_cast<cuDoubleComplex*>(b),
                                     n, w, reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()),
