@@ -317,6 +317,7 @@ struct AccRun {
   DeviceBuffer<C>& tmp2m;      // 2m x 2m in this precision (projection staging)
   int n, m, chunk;
   int mcheck = m;              // bands whose residuals decide convergence (guard bands excluded)
+  bool guarded = false;        // guard-band modes: may skip the separate metric normalisation
   double op_ms = 0;
   long long op_cols = 0;
   Tracer* tr = nullptr;
@@ -404,7 +405,47 @@ struct AccRun {
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.hx(), n, blk.small.get(), m, one, blk.HP.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.sx(), n, blk.small.get(), m, one, blk.SP.get(), n);
     mark("orth_gemm");
-    // S-metric normalisation
+    // In the guard-band modes, when the library's own pencil solver takes
+    // the Rayleigh-Ritz step, the separate S-metric normalisation is
+    // skipped: that solver Jacobi-scales the overlap and floors dependent
+    // pivots exactly like the metric step, so [X P] spans the same space
+    // and the Ritz pairs are the same.  The FP64 mode keeps the reference's
+    // metric step.
+    const bool skip_metric = guarded && ss.own && 2 * m <= SmallEigen::kOwnMaxOrder;
+    C* pu = skip_metric ? blk.P.get() : blk.PU.get();
+    C* hpu = skip_metric ? blk.HP.get() : blk.HPU.get();
+    C* spu = skip_metric ? blk.SP.get() : blk.SPU.get();
+    if (!skip_metric) normalise_metric(one, zero);
+    // Rayleigh-Ritz on Z = [X PU]
+    double2* hs = sc.hsub.get();
+    double2* ssb = sc.ssub.get();
+    if constexpr (sizeof(R) == 8) {
+      project_upper<R>(rt, n, m, blk.x(), pu, blk.hx(), hpu, hs, hs);
+      project_upper<R>(rt, n, m, blk.x(), pu, blk.sx(), spu, ssb, ssb);
+    } else {
+      project_upper<R>(rt, n, m, blk.x(), pu, blk.hx(), hpu, tmp2m.get(), hs);
+      project_upper<R>(rt, n, m, blk.x(), pu, blk.sx(), spu, tmp2m.get(), ssb);
+    }
+    mark("rr_gemm");
+    ss.hegvd(hs, ssb, 2 * m, sc.w.get(), m);
+    mark("hegvd");
+    to_r(hs, 2 * m, blk.Y.get(), 2 * m, 2 * m, m);
+    const C* ytop = blk.Y.get();
+    const C* ybot = blk.Y.get() + m;
+    int nx = blk.cur ^ 1;
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, ytop, 2 * m, zero, blk.X[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, pu, n, ybot, 2 * m, one, blk.X[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.hx(), n, ytop, 2 * m, zero, blk.HX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, hpu, n, ybot, 2 * m, one, blk.HX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, 2 * m, zero, blk.SX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, spu, n, ybot, 2 * m, one, blk.SX[nx].get(), n);
+    blk.cur = nx;
+    mark("rr_rot");
+  }
+
+  // S-metric normalisation of P, HP, SP into PU, HPU, SPU
+  // (src/half_cuda_iterative_solver.cuf:166-176)
+  void normalise_metric(cplx_t<R> one, cplx_t<R> zero) {
     double2* metric = sc.metric.get();
     if constexpr (sizeof(R) == 8) {
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.P.get(), n, blk.SP.get(), n, zero, metric, m);
@@ -426,31 +467,6 @@ struct AccRun {
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HP.get(), n, blk.small.get(), m, zero, blk.HPU.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.SP.get(), n, blk.small.get(), m, zero, blk.SPU.get(), n);
     mark("metric_rot");
-    // Rayleigh-Ritz on Z = [X PU]
-    double2* hs = sc.hsub.get();
-    double2* ssb = sc.ssub.get();
-    if constexpr (sizeof(R) == 8) {
-      project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.hx(), blk.HPU.get(), hs, hs);
-      project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.sx(), blk.SPU.get(), ssb, ssb);
-    } else {
-      project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.hx(), blk.HPU.get(), tmp2m.get(), hs);
-      project_upper<R>(rt, n, m, blk.x(), blk.PU.get(), blk.sx(), blk.SPU.get(), tmp2m.get(), ssb);
-    }
-    mark("rr_gemm");
-    ss.hegvd(hs, ssb, 2 * m, sc.w.get(), m);
-    mark("hegvd");
-    to_r(hs, 2 * m, blk.Y.get(), 2 * m, 2 * m, m);
-    const C* ytop = blk.Y.get();
-    const C* ybot = blk.Y.get() + m;
-    int nx = blk.cur ^ 1;
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, ytop, 2 * m, zero, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.PU.get(), n, ybot, 2 * m, one, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.hx(), n, ytop, 2 * m, zero, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HPU.get(), n, ybot, 2 * m, one, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, 2 * m, zero, blk.SX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.SPU.get(), n, ybot, 2 * m, one, blk.SX[nx].get(), n);
-    blk.cur = nx;
-    mark("rr_rot");
   }
 };
 
@@ -504,6 +520,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   AccRun<double> run64{ctx, ks, rt, b64, sc, ss, tmp64, n, m, cfg.block};
   run64.tr = &tracer;
   run64.mcheck = mreq;
+  run64.guarded = guarded;
 
   if (mixed) {
     // ---------------- FP32 phase
@@ -513,6 +530,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     AccRun<float> run32{ctx, ks, rt, b32, sc, ss, tmp32, n, m, cfg.block};
     run32.tr = &tracer;
     run32.mcheck = mreq;
+    run32.guarded = guarded;
     init_states_kernel<float2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b32.x(), n, n, m, sc.idx.get());
     ++rt.prof.launches;
     run32.apply(b32.x(), b32.hx(), b32.sx(), m);
