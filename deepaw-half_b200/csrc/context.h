@@ -67,6 +67,8 @@ struct Runtime {
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
   bool bf16x9 = false;   // cuBLAS offers FP32 emulation on BF16 tensor cores
+  bool tc_split = true;  // large complex FP32 GEMMs as split BF16 tensor-core GEMMs (blas_split.cu)
+  DeviceBuffer<unsigned char> split_a, split_b, split_c;   // their packed operands, grow-only
   Profile prof;
   Runtime();
   ~Runtime();

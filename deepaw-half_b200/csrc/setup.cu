@@ -38,6 +38,7 @@ Runtime::Runtime() {
   if (bf16x9 && cublasSetMathMode(blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) != CUBLAS_STATUS_SUCCESS) bf16x9 = false;
   HALF_CUDA(cudaEventCreate(&prof.a));
   HALF_CUDA(cudaEventCreate(&prof.b));
+  if (const char* sp = std::getenv("HALF_TC_SPLIT")) tc_split = std::string(sp) != "0";
 }
 
 int Profile::record(cudaStream_t s) {
