@@ -148,6 +148,8 @@ class CpuBaseline:
             self.cores = os.cpu_count() or 1
         self.w = w
         self.sysm = H.load_system(ch, po, w.encut, use_pbe=(w.xc == "pbe"), use_uspp=True)
+        from oracle.basis import build_basis
+        self.npw = build_basis(self.sysm.crystal, w.grid, w.encut, w.kpoints[0]).npw
 
     def measure(self, fp64_iterations, sample_s):
         from oracle import hamiltonian as H, acc
@@ -169,6 +171,14 @@ class CpuBaseline:
                 "sample": f"oracle FP64 acc restatement (numpy/scipy), {w.name} Gamma: operator preparation + "
                           f"{iters} iterations timed ({t_it * 1e3:.1f} ms/iteration), scaled to the "
                           f"{fp64_iterations} iterations the FP64 solve needs at this tolerance"}
+
+
+def workload_config(w, npw, args, nk, world, l2):
+    """The `config` object both arms print for the same workload."""
+    return {"workload": f"{w.name}: {w.nions} atoms, Gamma, {w.grid[0]}^3 box, {npw} plane waves, "
+                        f"{w.nbands} bands, PBE, MIMIC_US D_ij", "tol_eV": args.tol,
+            "block": args.block, "kpoints_per_rank": nk, "l2": l2,
+            "parallelism": f"k-point ownership x{world}" if world > 1 else "single GPU"}
 
 
 def cpu_baseline(w, ch, po, fp64_iterations, sample_s):
@@ -200,7 +210,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/k-point", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": f"{w.name} Gamma, {w.nbands} bands, tol {args.tol} eV", "l2": "n/a (host)"},
+            "config": workload_config(w, base.npw, args, len(owned(w.kpoints, 0, 1)), 1, "n/a (host)"),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "ms/k-point", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -337,12 +347,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "ms/k-point", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64/c128 (mixed: FP32 operator + BF16x9 GEMMs, FP64 refinement)",
+        "vs_baseline": None, "dtype": "c64/c128 (mixed: FP32 operator and GEMMs, FP64 small solves and refinement)",
         "data": "synthetic (seeded CHGCAR/POTCAR in the reference formats)",
-        "config": {"workload": f"{w.name}: {w.nions} atoms, Gamma, {w.grid[0]}^3 box, {npw[0]} plane waves, "
-                               f"{w.nbands} bands, PBE, MIMIC_US D_ij", "tol_eV": args.tol,
-                   "block": args.block, "kpoints_per_rank": nk, "l2": "flushed between steps (256 MB write)",
-                   "parallelism": f"k-point ownership x{world}" if world > 1 else "single GPU"},
+        "config": workload_config(w, npw[0], args, nk, world, "flushed between steps (256 MB write)"),
         "max_abs_d_eps_eV": max(errs) if errs else None,
         "per_step": [{"ms": round(t, 3), "iterations": i["iterations"], "fp64_iterations": i["fp64_iterations"]}
                      for t, i in zip(dev_ms, infos)],
