@@ -809,3 +809,145 @@ extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoint
     return HALF_SUCCESS;
   });
 }
+
+extern "C" int half_ionic_forces(half_handle handle, const double* output_density, int64_t n, double* ewald,
+                                 double* local, double* nlcc, double* harris, double* energies, char* error,
+                                 int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (output_density && n != ctx->nr()) {
+    export_error("output density size does not match the context's grid", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    if (output_density)
+      for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(output_density[i])) fail(kInvalidArgument, "output density must be finite");
+    IonicForces f;
+    ctx->last = SolveInfo();
+    begin_call(*ctx->rt);
+    ionic_forces_device(*ctx, output_density, false, ewald || energies, local || energies, nlcc != nullptr,
+                        harris != nullptr, f);
+    end_call(*ctx->rt, ctx->last);
+    if (ewald) std::copy(f.ewald.begin(), f.ewald.end(), ewald);
+    if (local) std::copy(f.local.begin(), f.local.end(), local);
+    if (nlcc) std::copy(f.nlcc.begin(), f.nlcc.end(), nlcc);
+    if (harris) std::copy(f.harris.begin(), f.harris.end(), harris);
+    if (energies) {
+      std::copy(f.ewald_energy, f.ewald_energy + 5, energies);
+      energies[5] = f.local_energy;
+    }
+    return HALF_SUCCESS;
+  });
+}
+
+extern "C" int half_output_density(half_handle handle, int nk, const double* kpoints, const double* kweights,
+                                   int nbands, int64_t ld, const HALF_C128* vectors, const double* occupations,
+                                   double* density, int64_t n, double* augmentation_charge, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || !kweights || nbands < 1 || !vectors || !occupations || !density) {
+    export_error("invalid output-density arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  if (n != ctx->nr()) {
+    export_error("density size does not match the context's grid", error, cap);
+    return HALF_ERROR_CAPACITY;
+  }
+  return guarded(error, cap, [&]() -> int {
+    for (int ik = 0; ik < nk; ++ik)
+      if (!finite3(kpoints + 3 * ik)) fail(kInvalidArgument, "k point must be finite");
+    cudaStream_t st = ctx->rt->stream;
+    std::vector<DeviceBuffer<double2>> dv(nk);
+    std::vector<const double2*> ptr(nk);
+    std::vector<long long> lds(nk);
+    for (int ik = 0; ik < nk; ++ik) {
+      const Basis b = build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoints + 3 * ik);
+      const long long npw = b.npw();
+      if (ld < npw) fail(kCapacity, "eigenvector leading dimension is too small");
+      dv[ik].resize((size_t)npw * nbands);
+      const HALF_C128* src = vectors + (size_t)ik * ld * nbands;
+      HALF_CUDA(cudaMemcpy2DAsync(dv[ik].get(), npw * sizeof(double2), src, ld * sizeof(double2),
+                                  npw * sizeof(double2), nbands, cudaMemcpyHostToDevice, st));
+      ptr[ik] = dv[ik].get();
+      lds[ik] = npw;
+    }
+    DeviceBuffer<double> out(ctx->nr());
+    double aug = 0;
+    ctx->last = SolveInfo();
+    begin_call(*ctx->rt);
+    output_density_device(*ctx, nk, kpoints, kweights, nbands, ptr, lds, occupations, out.get(), &aug);
+    end_call(*ctx->rt, ctx->last);
+    HALF_CUDA(cudaMemcpyAsync(density, out.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaStreamSynchronize(st));
+    if (augmentation_charge) *augmentation_charge = aug;
+    return HALF_SUCCESS;
+  });
+}
+
+extern "C" int half_forces(half_handle handle, int nk, const double* kpoints, const double* kweights, int nbands,
+                           double nelect, double sigma, int ismear, double* forces, double* components,
+                           double* output_density, double* energies, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || !kweights || nbands < 1 || !forces || !(sigma >= 0) || (ismear != -1 && ismear != 0)) {
+    export_error("invalid force arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    std::vector<SolveOutput> outs(nk);
+    std::vector<double> eig((size_t)nk * nbands);
+    for (int ik = 0; ik < nk; ++ik) {
+      outs[ik].keep_device = true;
+      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik]);
+      std::copy(outs[ik].eigenvalues.begin(), outs[ik].eigenvalues.end(), eig.begin() + (size_t)ik * nbands);
+    }
+    std::vector<double> occ;
+    double mu = 0, band = 0, entropy = 0;
+    compute_occupations(eig, nk, nbands, kweights, nelect, sigma, ismear, occ, mu, band, entropy);
+    if (sigma > 0)   // app/half_cli.F90:897
+      for (int ik = 0; ik < nk; ++ik)
+        if (occ[(size_t)ik * nbands + nbands - 1] > 1e-6)
+          fail(kInvalidArgument, "highest computed band is occupied; increase nbands");
+    const int nions = ctx->crystal.nions();
+    std::vector<double> nonlocal(3 * (size_t)nions, 0.0);
+    std::vector<const double2*> ptr(nk);
+    std::vector<long long> lds(nk);
+    for (int ik = 0; ik < nk; ++ik) {
+      auto ks = prepare_operator(*ctx, *ctx->rt, kpoints + 3 * ik, true, false);
+      nonlocal_forces_device(*ctx, *ks, outs[ik].dvectors.get(), ks->basis.npw(), nbands,
+                             eig.data() + (size_t)ik * nbands, occ.data() + (size_t)ik * nbands, kweights[ik],
+                             nonlocal.data());
+      ptr[ik] = outs[ik].dvectors.get();
+      lds[ik] = ks->basis.npw();
+    }
+    const long long n = ctx->nr();
+    DeviceBuffer<double> rho_out(n);
+    double aug = 0;
+    output_density_device(*ctx, nk, kpoints, kweights, nbands, ptr, lds, occ.data(), rho_out.get(), &aug);
+    IonicForces f;
+    ionic_forces_device(*ctx, rho_out.get(), true, true, true, true, true, f);
+    for (int i = 0; i < 3 * nions; ++i) forces[i] = f.ewald[i] + f.local[i] + nonlocal[i] + f.nlcc[i] + f.harris[i];
+    if (components) {
+      const std::vector<double>* parts[5] = {&f.ewald, &f.local, &nonlocal, &f.nlcc, &f.harris};
+      for (int c = 0; c < 5; ++c) std::copy(parts[c]->begin(), parts[c]->end(), components + (size_t)c * 3 * nions);
+    }
+    if (output_density) {
+      HALF_CUDA(cudaMemcpyAsync(output_density, rho_out.get(), sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                ctx->rt->stream));
+      HALF_CUDA(cudaStreamSynchronize(ctx->rt->stream));
+    }
+    if (energies) {
+      energies[0] = band;
+      energies[1] = entropy;
+      energies[2] = mu;
+      energies[3] = f.ewald_energy[0];
+      energies[4] = f.local_energy;
+      energies[5] = aug;
+    }
+    return HALF_SUCCESS;
+  });
+}

@@ -138,6 +138,31 @@ struct Context {
 void build_veff_device(Context& ctx);                 // setup.cu
 void build_dij_device(Context& ctx, bool gradient);   // setup.cu
 void fft3d_inplace(double2* data, const std::array<int, 3>& shape, int sign, cudaStream_t s);
+// Effective potential of a device density (C order, rho * Omega): veff = local + V_xc and,
+// when vxc is not null, V_xc alone (both C order, eV; src/half_potential.F90:31-93).
+// Synchronises s before returning.
+void build_potential(Context& ctx, cudaStream_t s, const double* charge_c, double* veff, double* vxc);
+void density_to_c_order(const double* f_order, double* c_order, const std::array<int, 3>& shape, cudaStream_t s);
+// freq = FFT_forward(real_c) / N over the box (the reference's fft3_forward then /n)
+void forward_transform(const double* real_c, double2* freq, const std::array<int, 3>& shape, cudaStream_t s);
+
+// ----------------------------------------------------------------- ion-position forces (ionforces.cu)
+struct IonicForces {
+  std::vector<double> ewald, local, nlcc, harris;   // nions * 3 each, eV/A (empty when not requested)
+  double ewald_energy[5] = {0, 0, 0, 0, 0};          // total, real, reciprocal, self, background
+  double local_energy = 0;
+};
+// output_f: the output density in file order (x fastest, rho * Omega), host or device memory;
+// null = the context's density.
+void ionic_forces_device(Context& ctx, const double* output_f, bool output_on_device, bool want_ewald,
+                         bool want_local, bool want_nlcc, bool want_harris, IonicForces& out);
+
+// ----------------------------------------------------------------- output density (density.cu)
+// density_f (device, n, file order) = smooth density of the states plus the augmentation density;
+// vectors[ik] (device, ld[ik] x nb column-major), occupations [nk][nb].
+void output_density_device(Context& ctx, int nk, const double* kpoints, const double* kweights, int nb,
+                           const std::vector<const double2*>& vectors, const std::vector<long long>& ld,
+                           const double* occupations, double* density_f, double* augmentation_charge);
 
 // ----------------------------------------------------------------- operator
 template <typename R>

@@ -160,6 +160,49 @@ __global__ void __launch_bounds__(512) k3_planes_to_sphere(const cplx_t<R>* __re
   }
 }
 
+// Density variant of k2_xlines: the block owns the box points (all i1, its
+// i2, its z tile) and runs the chunk's bands in order through the inverse x
+// transform, accumulating bw[b] |psi_b(r)|^2; the chunk total is added to
+// density (C order) once.  No atomics: each point has one owner.
+__global__ void __launch_bounds__(256) k2_density(const double2* __restrict__ work, int n1, int n2, int n3,
+                                                  int nplanes, const int* __restrict__ plane_xpos, AxisPlan ax,
+                                                  const double* __restrict__ bw, int nb,
+                                                  double* __restrict__ density) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* tw = reinterpret_cast<double2*>(smem_raw);
+  double2* X = tw + kMaxFFT;                                   // [i1][tz]
+  double* acc = reinterpret_cast<double*>(X + n1 * kXTile);    // [i1][tz]
+  int* xpos = reinterpret_cast<int*>(acc + n1 * kXTile);
+  const int tiles = (n3 + kXTile - 1) / kXTile;
+  const int i2 = blockIdx.x / tiles, z0 = (blockIdx.x - i2 * tiles) * kXTile;
+  const int nz = min(kXTile, n3 - z0);
+  fill_twiddles(tw, n1);
+  for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) acc[t] = 0.0;
+  for (int t = threadIdx.x; t < nplanes; t += blockDim.x) xpos[t] = plane_xpos[t];
+  const long long npl = (long long)n2 * n3;
+  for (int b = 0; b < nb; ++b) {
+    for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) X[t] = czero<double2>();
+    __syncthreads();
+    const double2* base = work + (long long)b * nplanes * npl + (long long)i2 * n3 + z0;
+    for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
+      int jj = t / kXTile, c = t - jj * kXTile;
+      if (c < nz) X[xpos[jj] * kXTile + c] = base[jj * npl + c];
+    }
+    __syncthreads();
+    fft_pencils<true, double2, double>(X, kXTile, 1, kXTile, ax.plan, tw, +1);
+    const double w = bw[b];
+    for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) {
+      const double2 v = X[t];
+      acc[t] += w * (v.x * v.x + v.y * v.y);
+    }
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) {
+    int i1 = t / kXTile, c = t - i1 * kXTile;
+    if (c < nz) density[((long long)i1 * n2 + i2) * n3 + z0 + c] += acc[t];
+  }
+}
+
 // dy[:,b] = blockdiag(D_atom) coeff[:,b], qy[:,b] = blockdiag(Q_species) coeff[:,b]
 // (src/half_cuda_assembly.cuf:220-237)
 template <typename R>
@@ -498,6 +541,32 @@ void apply_nonlocal(Runtime& rt, KOperator<R>& op, const cplx_t<R>* x, long long
 
 template void apply_hs<double>(Context&, KOperatorSet&, const double2*, long long, int, double2*, double2*, int);
 template void apply_hs<float>(Context&, KOperatorSet&, const float2*, long long, int, float2*, float2*, int);
+
+void accumulate_band_density(KOperatorSet& ks, const double2* x, long long ld, int nb, const double* bw,
+                             double* density_c, int chunk) {
+  KOperator<double>& op = pick<double>(ks);
+  cudaStream_t s = ks.rt->stream;
+  if (nb <= 0) return;
+  chunk = std::max(1, std::min(chunk, nb));
+  if (op.work_chunk < chunk) {
+    op.work.resize((size_t)chunk * op.nplanes * op.n2 * op.n3);
+    op.work_chunk = chunk;
+  }
+  const size_t psm = plane_smem<double>(op.n2, op.n3);
+  const size_t dsm = xline_smem<double>(op.n1, op.nplanes) + size_t(op.n1) * kXTile * sizeof(double);
+  raise_smem_limit(k2_density, dsm);
+  const int tiles = (op.n3 + kXTile - 1) / kXTile;
+  for (int b0 = 0; b0 < nb; b0 += chunk) {
+    const int nbc = std::min(chunk, nb - b0);
+    k1_sphere_to_planes<double><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
+        x, ld, b0, op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(),
+        op.row_list.get(), op.ay, op.az, op.work.get());
+    k2_density<<<op.n2 * tiles, 256, dsm, s>>>(op.work.get(), op.n1, op.n2, op.n3, op.nplanes, op.plane_xpos.get(),
+                                                op.ax, bw + b0, nbc, density_c);
+    ks.rt->prof.launches += 2;
+  }
+  HALF_LAUNCH("band density");
+}
 
 // Projector matrix of the prepared k point (used by the dense path and forces).
 const double2* projector_matrix64(KOperatorSet& ks) { return pick<double>(ks).B.get(); }

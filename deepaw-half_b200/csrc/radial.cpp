@@ -59,31 +59,6 @@ std::vector<double> radial_weights(const std::vector<double>& r) {
   return w;
 }
 
-// src/half_uspp.F90:307-319
-double sph_bessel(int l, double x) {
-  if (std::fabs(x) < l + 2) {
-    double den = 1;
-    for (int i = 1; i <= l; ++i) den *= 2 * i + 1;
-    double x2 = x * x, term = std::pow(x, l) / den, v = term;
-    for (int k = 0; k <= 30; ++k) {
-      term = -term * x2 / (2.0 * (k + 1) * (2 * l + 2 * k + 3));
-      v += term;
-      if (std::fabs(term) < 1e-16 * std::max(1.0, std::fabs(v))) break;
-    }
-    return v;
-  }
-  double jm = std::sin(x) / x;
-  if (l == 0) return jm;
-  double j = std::sin(x) / (x * x) - std::cos(x) / x;
-  if (l == 1) return j;
-  for (int n = 1; n <= l - 1; ++n) {
-    double jn = (2 * n + 1) * j / x - jm;
-    jm = j;
-    j = jn;
-  }
-  return j;
-}
-
 double sph_bessel_deriv(int l, double x) {
   if (l == 0) return -sph_bessel(1, x);
   return sph_bessel(l - 1, x) - (l + 1) / x * sph_bessel(l, x);
@@ -211,6 +186,7 @@ QdepTables build_qdep_tables(const Potcar& pot) {
   for (int l = 0; l <= t.lmax; ++l) {
     double z1 = bessel_root(l, 1), z2 = bessel_root(l, 2), c1, c2;
     compensation_coefficients(l, pot.paw_rmax, z1, z2, c1, c2);
+    t.shape_coeff.insert(t.shape_coeff.end(), {z1, z2, c1, c2});
     for (int ir = 0; ir < t.nrad; ++ir) {
       double r = pot.rgrid[ir];
       if (r <= pot.paw_rmax)

@@ -82,7 +82,36 @@ struct QdepTables {
   std::vector<double> yweight;      // [ip][k]
   std::vector<double> dion_lm;      // [a][b]
   std::vector<double> qij_lm;       // [a][b]
+  // g_l(r) = c1 j_l(z1 r / rc) + c2 j_l(z2 r / rc) for r <= paw_rmax
+  // (src/half_uspp.F90:163-171): [l][4] = {z1, z2, c1, c2}
+  std::vector<double> shape_coeff;
 };
+
+// Spherical Bessel j_l (src/half_uspp.F90:307-319): power series below
+// x = l + 2, upward recurrence above.
+HALF_HD inline double sph_bessel(int l, double x) {
+  if (fabs(x) < l + 2) {
+    double den = 1;
+    for (int i = 1; i <= l; ++i) den *= 2 * i + 1;
+    double x2 = x * x, term = pow(x, double(l)) / den, v = term;
+    for (int k = 0; k <= 30; ++k) {
+      term = -term * x2 / (2.0 * (k + 1) * (2 * l + 2 * k + 3));
+      v += term;
+      if (fabs(term) < 1e-16 * fmax(1.0, fabs(v))) break;
+    }
+    return v;
+  }
+  double jm = sin(x) / x;
+  if (l == 0) return jm;
+  double j = sin(x) / (x * x) - cos(x) / x;
+  if (l == 1) return j;
+  for (int n = 1; n <= l - 1; ++n) {
+    double jn = (2 * n + 1) * j / x - jm;
+    jm = j;
+    j = jn;
+  }
+  return j;
+}
 
 struct Potcar;
 QdepTables build_qdep_tables(const Potcar& pot);

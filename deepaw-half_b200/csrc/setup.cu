@@ -15,6 +15,7 @@
 #include <string>
 
 #include "context.h"
+#include "grid.cuh"
 
 namespace hb {
 
@@ -153,24 +154,6 @@ void fft3d_inplace(double2* data, const std::array<int, 3>& shape, int sign, cud
 
 namespace {
 
-struct Grid3 {
-  int n1, n2, n3;
-  double rec[9];
-};
-
-__device__ __forceinline__ void gvector(long long idx, const Grid3& g, double& qx, double& qy, double& qz) {
-  int i3 = int(idx % g.n3);
-  long long t = idx / g.n3;
-  int i2 = int(t % g.n2);
-  int i1 = int(t / g.n2);
-  int k1 = i1 <= (g.n1 - 1) / 2 ? i1 : i1 - g.n1;
-  int k2 = i2 <= (g.n2 - 1) / 2 ? i2 : i2 - g.n2;
-  int k3 = i3 <= (g.n3 - 1) / 2 ? i3 : i3 - g.n3;
-  qx = k1 * g.rec[0] + k2 * g.rec[3] + k3 * g.rec[6];
-  qy = k1 * g.rec[1] + k2 * g.rec[4] + k3 * g.rec[7];
-  qz = k1 * g.rec[2] + k2 * g.rec[5] + k3 * g.rec[8];
-}
-
 __global__ void reorder_f_to_c_kernel(const double* in, double* out, int n1, int n2, int n3) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   long long n = (long long)n1 * n2 * n3;
@@ -235,14 +218,18 @@ __global__ void extract_real_kernel(const double2* in, double* out, long long n)
   if (i < n) out[i] = in[i].x;
 }
 
-// PZ81 LDA (src/half_cuda_potential.cuf:236-259)
+// PZ81 LDA (src/half_cuda_potential.cuf:236-259); vxc in eV.
 __global__ void lda_kernel(const double* charge, const double* core, const double* local_r, double* veff,
-                           long long n, double volume) {
+                           double* vxc, long long n, double volume) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double density = (charge[i] + core[i]) / volume;
   double rhoau = density * kAutoa * kAutoa * kAutoa;
-  if (rhoau <= 1.0e-30) { veff[i] = local_r[i]; return; }
+  if (rhoau <= 1.0e-30) {
+    veff[i] = local_r[i];
+    vxc[i] = 0.0;
+    return;
+  }
   double rs = cbrt(3.0 / (4 * kPi * rhoau));
   double vx = -(4.0 / 3.0) * 0.4582 / rs, vc;
   if (rs >= 1) {
@@ -253,7 +240,9 @@ __global__ void lda_kernel(const double* charge, const double* core, const doubl
     double lnrs = log(rs);
     vc = 0.0311 * lnrs + (-0.048 - 0.0311 / 3) + (2.0 / 3.0) * 0.002 * rs * lnrs + (-0.0232 - 0.002) * rs / 3;
   }
-  veff[i] = local_r[i] + (vx + vc) * kHatoev;
+  const double v = (vx + vc) * kHatoev;
+  vxc[i] = v;
+  veff[i] = local_r[i] + v;
 }
 
 __device__ double pw92_ec(double rs) {
@@ -336,30 +325,50 @@ __global__ void subtract_divergence_kernel(const double2* work, double* fn, long
 }
 
 __global__ void finish_pbe_kernel(const double* density, const double* local_r, const double* fn, double* veff,
-                                  long long n) {
+                                  double* vxc, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double v = density[i] <= 1.0e-20 ? 0.0 : fn[i];
-  veff[i] = local_r[i] + v * kHatoev;
+  const double v = (density[i] <= 1.0e-20 ? 0.0 : fn[i]) * kHatoev;
+  vxc[i] = v;
+  veff[i] = local_r[i] + v;
 }
-
-int blocks_for(long long n, int t = 256) { return ceil_div(n, t); }
 
 }  // namespace
 
-void build_veff_device(Context& ctx) {
-  cudaStream_t s = ctx.rt->stream;
+Grid3 charge_grid(const Context& ctx) {
   const auto& sh = ctx.charge.shape;
-  const long long n = ctx.nr();
   Grid3 g{sh[0], sh[1], sh[2], {}};
   auto rec = ctx.crystal.reciprocal();
   for (int i = 0; i < 9; ++i) g.rec[i] = rec[i];
+  return g;
+}
+
+void density_to_c_order(const double* f_order, double* c_order, const std::array<int, 3>& shape, cudaStream_t s) {
+  const long long n = (long long)shape[0] * shape[1] * shape[2];
+  reorder_f_to_c_kernel<<<blocks_for(n), 256, 0, s>>>(f_order, c_order, shape[0], shape[1], shape[2]);
+  HALF_LAUNCH("reorder density");
+}
+
+void forward_transform(const double* real_c, double2* freq, const std::array<int, 3>& shape, cudaStream_t s) {
+  const long long n = (long long)shape[0] * shape[1] * shape[2];
+  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(real_c, freq, n, 1.0 / double(n));
+  HALF_LAUNCH("real to complex");
+  fft3d_inplace(freq, shape, -1, s);
+}
+
+void build_potential(Context& ctx, cudaStream_t s, const double* charge, double* veff_out, double* vxc_out) {
+  const auto& sh = ctx.charge.shape;
+  const long long n = ctx.nr();
+  const Grid3 g = charge_grid(ctx);
   const double vol = ctx.crystal.volume();
-  DeviceBuffer<double> raw(n), charge(n), local_r(n), core_r(n);
+  DeviceBuffer<double> local_r(n), core_r(n), vxc_scratch;
+  double* vxc = vxc_out;
+  if (!vxc) {
+    vxc_scratch.resize(n);
+    vxc = vxc_scratch.get();
+  }
   DeviceBuffer<double2> work(n), rho_g(n), local_g(n), core_g(n);
-  raw.upload(ctx.charge.values, s);
-  reorder_f_to_c_kernel<<<blocks_for(n), 256, 0, s>>>(raw.get(), charge.get(), sh[0], sh[1], sh[2]);
-  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), rho_g.get(), n, 1.0 / double(n));
+  real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(charge, rho_g.get(), n, 1.0 / double(n));
   fft3d_inplace(rho_g.get(), sh, -1, s);
   hartree_kernel<<<blocks_for(n), 256, 0, s>>>(rho_g.get(), local_g.get(), core_g.get(), g, vol);
   HALF_LAUNCH("hartree");
@@ -396,14 +405,13 @@ void build_veff_device(Context& ctx) {
   extract_real_kernel<<<blocks_for(n), 256, 0, s>>>(local_g.get(), local_r.get(), n);
   fft3d_inplace(core_g.get(), sh, +1, s);
   extract_real_kernel<<<blocks_for(n), 256, 0, s>>>(core_g.get(), core_r.get(), n);
-  ctx.veff.resize(n);
   if (!ctx.use_pbe) {
-    lda_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), core_r.get(), local_r.get(), ctx.veff.get(), n, vol);
+    lda_kernel<<<blocks_for(n), 256, 0, s>>>(charge, core_r.get(), local_r.get(), veff_out, vxc, n, vol);
     HALF_LAUNCH("lda");
   } else {
     DeviceBuffer<double> density(n), sigma(n), grad(3 * n), fn(n), fs(n);
     DeviceBuffer<double2> freq(n), deriv(n);
-    pbe_density_kernel<<<blocks_for(n), 256, 0, s>>>(charge.get(), core_r.get(), density.get(), freq.get(), n, vol);
+    pbe_density_kernel<<<blocks_for(n), 256, 0, s>>>(charge, core_r.get(), density.get(), freq.get(), n, vol);
     fft3d_inplace(freq.get(), sh, -1, s);
     for (int a = 0; a < 3; ++a) {
       spectral_derivative_kernel<<<blocks_for(n), 256, 0, s>>>(freq.get(), deriv.get(), g, a);
@@ -418,11 +426,21 @@ void build_veff_device(Context& ctx) {
       fft3d_inplace(deriv.get(), sh, +1, s);
       subtract_divergence_kernel<<<blocks_for(n), 256, 0, s>>>(deriv.get(), fn.get(), n);
     }
-    finish_pbe_kernel<<<blocks_for(n), 256, 0, s>>>(density.get(), local_r.get(), fn.get(), ctx.veff.get(), n);
+    finish_pbe_kernel<<<blocks_for(n), 256, 0, s>>>(density.get(), local_r.get(), fn.get(), veff_out, vxc, n);
     HALF_LAUNCH("pbe");
-    HALF_CUDA(cudaStreamSynchronize(s));
   }
+  // the scratch above is released on return: finish its users first
   HALF_CUDA(cudaStreamSynchronize(s));
+}
+
+void build_veff_device(Context& ctx) {
+  cudaStream_t s = ctx.rt->stream;
+  const long long n = ctx.nr();
+  DeviceBuffer<double> raw(n), charge(n);
+  raw.upload(ctx.charge.values, s);
+  density_to_c_order(raw.get(), charge.get(), ctx.charge.shape, s);
+  ctx.veff.resize(n);
+  build_potential(ctx, s, charge.get(), ctx.veff.get(), nullptr);
 }
 
 // ------------------------------------------------------------------ QDEP

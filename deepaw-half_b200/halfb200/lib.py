@@ -89,6 +89,11 @@ _SIGS = {
     "half_nonlocal_forces": (C.c_int, [C.c_int64, _P, C.c_int, C.c_int64, _P, _P, _P, C.c_double, _P] + _ERR),
     "half_band_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P,
                                    _P] + _ERR),
+    "half_ionic_forces": (C.c_int, [C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P] + _ERR),
+    "half_output_density": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_int64, _P, _P, _P, C.c_int64, _P]
+                            + _ERR),
+    "half_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P, _P]
+                    + _ERR),
 }
 
 
@@ -312,3 +317,61 @@ class Context:
         _check(self.lib.half_band_forces(self.handle, len(ks), _ptr(ks), _ptr(w), nbands, float(nelect), float(sigma),
                                          int(ismear), _ptr(f), _ptr(eig), _ptr(occ), _ptr(en), err, 512), err)
         return dict(forces=f, eigenvalues=eig, occupations=occ, band_energy=en[0], entropy=en[1], mu=en[2])
+
+    def ionic_forces(self, output_density=None):
+        """Ewald, local, NLCC and Harris forces (each (nions, 3), eV/A) and the
+        Ewald / local energies; output_density in file order (x fastest,
+        rho * Omega), None = the context's own density."""
+        err = self._err()
+        d = None
+        n = 0
+        if output_density is not None:
+            d = np.ascontiguousarray(np.asarray(output_density, dtype=np.float64).reshape(-1))
+            n = d.size
+        out = {k: np.zeros((self.nions, 3)) for k in ("ewald", "local", "nlcc", "harris")}
+        en = np.zeros(6)
+        _check(self.lib.half_ionic_forces(self.handle, _ptr(d) if d is not None else None, n, _ptr(out["ewald"]),
+                                          _ptr(out["local"]), _ptr(out["nlcc"]), _ptr(out["harris"]), _ptr(en),
+                                          err, 512), err)
+        out.update(ewald_energy=en[0], ewald_real=en[1], ewald_reciprocal=en[2], ewald_self=en[3],
+                   ewald_background=en[4], local_energy=en[5])
+        return out
+
+    def grid_size(self):
+        return int(np.prod(self.grid))
+
+    def output_density(self, kpoints, weights, vectors, occupations):
+        """Smooth + augmentation density (file order) of given states: vectors is a
+        list of (npw_k, nbands) arrays, occupations (nk, nbands)."""
+        err = self._err()
+        ks = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        nb = int(np.asarray(vectors[0]).shape[1])
+        ld = max(int(np.asarray(v).shape[0]) for v in vectors)
+        block = np.zeros((len(ks), nb, ld), dtype=np.complex128)      # per k: column-major ld x nb
+        for ik, v in enumerate(vectors):
+            v = np.asarray(v, dtype=np.complex128)
+            block[ik, :, :v.shape[0]] = v.T
+        occ = np.ascontiguousarray(np.asarray(occupations, dtype=np.float64).reshape(len(ks), nb))
+        n = self.grid_size()
+        rho = np.zeros(n)
+        aug = C.c_double(0.0)
+        _check(self.lib.half_output_density(self.handle, len(ks), _ptr(ks), _ptr(w), nb, ld, _ptr(block), _ptr(occ),
+                                            _ptr(rho), n, C.byref(aug), err, 512), err)
+        return rho, aug.value
+
+    def forces(self, kpoints, weights, nbands, nelect, sigma, ismear=-1):
+        """The analytic --forces workload: total force, its five components, the
+        output density and the energies."""
+        err = self._err()
+        ks = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        f = np.zeros((self.nions, 3))
+        comp = np.zeros((5, self.nions, 3))
+        rho = np.zeros(self.grid_size())
+        en = np.zeros(6)
+        _check(self.lib.half_forces(self.handle, len(ks), _ptr(ks), _ptr(w), int(nbands), float(nelect), float(sigma),
+                                    int(ismear), _ptr(f), _ptr(comp), _ptr(rho), _ptr(en), err, 512), err)
+        return dict(forces=f, ewald=comp[0], local=comp[1], **{"nonlocal": comp[2]}, nlcc=comp[3], harris=comp[4],
+                    output_density=rho, band_energy=en[0], entropy=en[1], mu=en[2], ewald_energy=en[3],
+                    local_energy=en[4], augmentation_charge=en[5])

@@ -48,6 +48,7 @@ class SpeciesSpec:
     amp: float = 2.0
     rloc: float = 1.0    # erf width of the ionic local potential
     v0: float = 20.0     # short-range repulsive Gaussian (eV)
+    core: float = 0.0    # partial core charge (electrons) for the non-linear core correction; 0 = none
 
 
 @dataclass
@@ -112,11 +113,17 @@ SI = SpeciesSpec("Si", 4.0, [0, 0, 1, 1])
 
 def workload(name, seed=None):
     """Build one of the named synthetic workloads (positions, box, k set)."""
-    base = {"si2": 11, "hfo2": 12, "si64": 13, "si64d": 14, "si216v": 15}
+    base = {"si2": 11, "hfo2": 12, "si64": 13, "si64d": 14, "si216v": 15, "si2c": 16}
     if name not in base:
         raise KeyError(name)
     seed = 20261203 + base[name] if seed is None else seed
     rng = np.random.default_rng(seed)
+    if name == "si2c":   # the Si cell with a partial core (non-linear core correction), displaced atoms
+        a = 5.43
+        lat = a / 2 * np.array([[0, 1, 1], [1, 0, 1], [1, 1, 0]], dtype=float)
+        spec = SpeciesSpec("Si", 4.0, [0, 0, 1, 1], core=1.5)
+        return Workload(name, lat, [spec], [2], np.array([[0.01, -0.02, 0.015], [.25, .26, .24]]), (24, 24, 24),
+                        400.0, "pbe", 16, np.zeros((1, 3)), np.ones(1), seed=seed)
     if name == "si2":
         a = 5.43
         lat = a / 2 * np.array([[0, 1, 1], [1, 0, 1], [1, 1, 0]], dtype=float)
@@ -191,6 +198,9 @@ def species_dataset(spec, rng):
     a_sr = 0.7
     local = coul + spec.v0 * np.pi ** 1.5 * a_sr ** 3 * np.exp(-qloc ** 2 * a_sr ** 2 / 4)
     psprho = spec.zval * np.exp(-qloc ** 2 * 0.3)
+    # partial core density in the POTCAR's reciprocal convention (value at q=0 = core electrons);
+    # deterministic, so datasets without a core draw the same random numbers as before
+    pspcor = spec.core * np.exp(-qloc ** 2 * 0.15) if spec.core > 0 else None
     rgrid = 0.002 * np.exp(np.arange(NMAX) * math.log(2.0 / 0.002) / (NMAX - 1))
     wps = np.zeros((NMAX, nch)); wae = np.zeros((NMAX, nch))
     seen = {}
@@ -200,7 +210,7 @@ def species_dataset(spec, rng):
         bump = np.where(rgrid < PAW_RMAX, rgrid ** (l + 1) * (1 - (rgrid / PAW_RMAX) ** 2) ** 2, 0.0)
         wae[:, ich] = wps[:, ich] + rng.uniform(-0.3, 0.3) * bump
     return dict(element=spec.element, zval=spec.zval, lps=lps, pspnl=pspnl, psprnl=psprnl, dion=dion,
-                qpaw=qpaw, local=local, psprho=psprho, rgrid=rgrid, wps=wps, wae=wae)
+                qpaw=qpaw, local=local, psprho=psprho, pspcor=pspcor, rgrid=rgrid, wps=wps, wae=wae)
 
 
 def _block(values, per_line=5):
@@ -225,8 +235,10 @@ def potcar_text(ds):
            f"  {PSP_GMAX:.16f}",
            _block(ds["local"]),
            " gradient corrections used for XC",
-           "     2",
-           " atomic pseudo charge-density",
+           "     2"]
+    if ds.get("pspcor") is not None:
+        out += [" core charge-density (partial)", _block(ds["pspcor"])]
+    out += [" atomic pseudo charge-density",
            _block(ds["psprho"]),
            f"  {PSPNL_GMAX:.16f}"]
     lps = ds["lps"]

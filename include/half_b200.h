@@ -140,6 +140,63 @@ int half_band_forces(half_handle handle, int nk, const double *kpoints,
                      double *eigenvalues_eV, double *occupations,
                      double *energies, char *error, int error_capacity);
 
+/* The ion-position force terms that the reference's --forces path adds to
+ * the non-local force (app/half_cli.F90:947-955), on the GPU.  Each force
+ * output is [nions][3] (eV/A, atom-major), overwritten; NULL skips the term:
+ *   ewald   ion-ion Ewald force (src/half_energy.F90:164-210);
+ *   local   local ionic force on the output density
+ *           (src/half_local_forces.F90:11-56);
+ *   nlcc    non-linear core correction force with the XC potential of the
+ *           context's density (:58-100); zero without a partial core;
+ *   harris  frozen-input Harris response from the context's density to the
+ *           output density (:129-161); zero without a partial core.
+ * output_density: n values on the context's grid in the CHGCAR convention
+ * (x fastest, rho * Omega), normally the smooth plus augmentation density of
+ * the solved states; NULL = the context's own density (Harris is then zero).
+ * energies (NULL to skip) [6] = {Ewald total, real-space, reciprocal, self,
+ * background (src/half_energy.F90:122-162), local ionic energy on the output
+ * density}. */
+int half_ionic_forces(half_handle handle, const double *output_density,
+                      int64_t n, double *ewald, double *local, double *nlcc,
+                      double *harris, double *energies, char *error,
+                      int error_capacity);
+
+/* Output density of given states on the GPU: the smooth density
+ * sum_k w_k sum_n f_nk |psi_nk(r)|^2 (src/half_local_forces.F90:102-127) plus
+ * the MIMIC_US augmentation density of the occupancies
+ * rho_ij = sum w f Re(conj(c_i) c_j), c = B^H psi (src/half_uspp.F90:26-111).
+ * vectors: nk consecutive blocks of ld x nbands (column-major, ld >= npw of
+ * every k point); occupations [nk][nbands] (bands with f = 0 contribute
+ * nothing).  density: n values on the context's grid in the CHGCAR convention
+ * (x fastest, rho * Omega), overwritten; n must equal the grid size, else
+ * HALF_ERROR_CAPACITY.  augmentation_charge (NULL to skip): the augmentation's
+ * contribution to the grid average, the reference's integrated_charge. */
+int half_output_density(half_handle handle, int nk, const double *kpoints,
+                        const double *kweights, int nbands, int64_t ld,
+                        const HALF_C128 *vectors, const double *occupations,
+                        double *density, int64_t n,
+                        double *augmentation_charge, char *error,
+                        int error_capacity);
+
+/* The reference's analytic --forces workload end to end on the GPU
+ * (app/half_cli.F90:895-955): solve nk k points with the context's solver,
+ * occupations (as half_band_forces), the non-local force, the output density
+ * (as half_output_density), then the ion-position terms (as
+ * half_ionic_forces with that density).
+ *   forces [nions][3] = Ewald + local + non-local + NLCC + Harris, eV/A;
+ *   components (NULL to skip) [5][nions][3] = {Ewald, local, non-local, NLCC,
+ *     Harris};
+ *   output_density (NULL to skip) [n] as half_output_density;
+ *   energies (NULL to skip) [6] = {band energy, entropy term, chemical
+ *     potential, Ewald energy, local ionic energy, augmentation charge}.
+ * With sigma > 0 an occupied highest band (f > 1e-6 at any k) is an
+ * HALF_ERROR_INVALID_ARGUMENT, as in the reference CLI. */
+int half_forces(half_handle handle, int nk, const double *kpoints,
+                const double *kweights, int nbands, double nelect,
+                double sigma, int ismear, double *forces, double *components,
+                double *output_density, double *energies, char *error,
+                int error_capacity);
+
 #ifdef __cplusplus
 }
 #endif
