@@ -951,3 +951,61 @@ extern "C" int half_forces(half_handle handle, int nk, const double* kpoints, co
     return HALF_SUCCESS;
   });
 }
+
+extern "C" int half_pack_vasp_waves(half_handle handle, int nk, const double* kpoints, int nbands, int64_t ld,
+                                    const HALF_C128* vectors, float* packed, int64_t capacity, int* npws,
+                                    int64_t* offsets, char* error, int cap) {
+  clear_error(error, cap);
+  Context* ctx = lookup(handle);
+  if (!ctx) return bad_handle(error, cap);
+  if (nk < 1 || !kpoints || nbands < 1 || !npws || !offsets || (packed && !vectors) || capacity < 0) {
+    export_error("invalid wave-export arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    std::vector<Basis> bases;
+    int64_t total = 0;
+    for (int ik = 0; ik < nk; ++ik) {
+      if (!finite3(kpoints + 3 * ik)) fail(kInvalidArgument, "k point must be finite");
+      bases.push_back(build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoints + 3 * ik));
+      if (bases.back().npw() > ld) fail(kCapacity, "eigenvector leading dimension is smaller than a k point's basis");
+      npws[ik] = int(bases.back().npw());
+      offsets[ik] = total;
+      total += 2 * int64_t(npws[ik]) * nbands;
+    }
+    if (!packed) return HALF_SUCCESS;   // size query
+    if (capacity < total) fail(kCapacity, "packed buffer is smaller than 2 * nbands * sum(npw)");
+    Runtime& rt = *ctx->rt;
+    cudaStream_t st = rt.stream;
+    const bool vec_dev = device_pointer(vectors), out_dev = device_pointer(packed);
+    ctx->last = SolveInfo();
+    begin_call(rt);
+    for (int ik = 0; ik < nk; ++ik) {
+      const int npw = npws[ik];
+      const double2* src = reinterpret_cast<const double2*>(vectors) + (size_t)ik * ld * nbands;
+      DeviceBuffer<double2> dv;
+      long long sld = ld;
+      if (!vec_dev) {
+        dv.resize((size_t)npw * nbands);
+        HALF_CUDA(cudaMemcpy2DAsync(dv.get(), npw * sizeof(double2), src, ld * sizeof(double2), npw * sizeof(double2),
+                                    nbands, cudaMemcpyHostToDevice, st));
+        src = dv.get();
+        sld = npw;
+      }
+      float2* dst = reinterpret_cast<float2*>(packed + offsets[ik]);
+      DeviceBuffer<float2> dout;
+      if (!out_dev) {
+        dout.resize((size_t)npw * nbands);
+        dst = dout.get();
+      }
+      pack_vasp_device(rt, src, sld, npw, nbands, vasp_order(bases[ik]), dst);
+      if (!out_dev) {
+        HALF_CUDA(cudaMemcpyAsync(packed + offsets[ik], dout.get(), sizeof(float2) * npw * nbands,
+                                  cudaMemcpyDeviceToHost, st));
+        HALF_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+    end_call(rt, ctx->last);
+    return HALF_SUCCESS;
+  });
+}

@@ -157,6 +157,13 @@ struct IonicForces {
 void ionic_forces_device(Context& ctx, const double* output_f, bool output_on_device, bool want_ewald,
                          bool want_local, bool want_nlcc, bool want_harris, IonicForces& out);
 
+// ----------------------------------------------------------------- VASP wave export (export.cu)
+// Basis indices in VASP's plane-wave order (the box's x-fastest order).
+std::vector<int> vasp_order(const Basis& b);
+// out (device, nb x npw float2, band-major) = FP32 coefficients vec[b*ld + order[g]].
+void pack_vasp_device(Runtime& rt, const double2* vec, long long ld, int npw, int nb, const std::vector<int>& order,
+                      float2* out);
+
 // ----------------------------------------------------------------- output density (density.cu)
 // density_f (device, n, file order) = smooth density of the states plus the augmentation density;
 // vectors[ik] (device, ld[ik] x nb column-major), occupations [nk][nb].

@@ -10,7 +10,7 @@ struct SmallEigen {
   // (order 320: 4.7 against 5.9 ms; order 1080: 20 against 37 ms).
   static constexpr int kOwnMaxOrder = 164;
   int cap = 0;
-  DeviceBuffer<double> d, e, Z, scratch;
+  DeviceBuffer<double> d, e, Z, scratch, lam;
   DeviceBuffer<double2> tau, V, work;
   DeviceBuffer<int> info;   // zhetrd status (reports illegal arguments only)
   void reserve(Runtime& rt, int nmax);

@@ -92,6 +92,8 @@ _SIGS = {
     "half_ionic_forces": (C.c_int, [C.c_int64, _P, C.c_int64, _P, _P, _P, _P, _P] + _ERR),
     "half_output_density": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_int64, _P, _P, _P, C.c_int64, _P]
                             + _ERR),
+    "half_pack_vasp_waves": (C.c_int, [C.c_int64, C.c_int, _P, C.c_int, C.c_int64, _P, _P, C.c_int64, _P, _P]
+                             + _ERR),
     "half_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P, _P]
                     + _ERR),
 }
@@ -359,6 +361,26 @@ class Context:
         _check(self.lib.half_output_density(self.handle, len(ks), _ptr(ks), _ptr(w), nb, ld, _ptr(block), _ptr(occ),
                                             _ptr(rho), n, C.byref(aug), err, 512), err)
         return rho, aug.value
+
+    def pack_vasp_waves(self, kpoints, vectors):
+        """VASP-ordered single-precision coefficients: (packed float32, npws, offsets);
+        vectors is a list of (npw_k, nbands) arrays (host memory)."""
+        err = self._err()
+        ks = np.ascontiguousarray(np.asarray(kpoints, dtype=np.float64).reshape(-1, 3))
+        nb = int(np.asarray(vectors[0]).shape[1])
+        ld = max(int(np.asarray(v).shape[0]) for v in vectors)
+        block = np.zeros((len(ks), nb, ld), dtype=np.complex128)
+        for ik, v in enumerate(vectors):
+            v = np.asarray(v, dtype=np.complex128)
+            block[ik, :, :v.shape[0]] = v.T
+        npws = np.zeros(len(ks), dtype=np.int32)
+        offsets = np.zeros(len(ks), dtype=np.int64)
+        _check(self.lib.half_pack_vasp_waves(self.handle, len(ks), _ptr(ks), nb, ld, _ptr(block), None, 0, _ptr(npws),
+                                             _ptr(offsets), err, 512), err)
+        packed = np.zeros(int(2 * nb * npws.astype(np.int64).sum()), dtype=np.float32)
+        _check(self.lib.half_pack_vasp_waves(self.handle, len(ks), _ptr(ks), nb, ld, _ptr(block), _ptr(packed),
+                                             packed.size, _ptr(npws), _ptr(offsets), err, 512), err)
+        return packed, npws, offsets
 
     def forces(self, kpoints, weights, nbands, nelect, sigma, ismear=-1):
         """The analytic --forces workload: total force, its five components, the

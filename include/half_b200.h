@@ -197,6 +197,22 @@ int half_forces(half_handle handle, int nk, const double *kpoints,
                 double *output_density, double *energies, char *error,
                 int error_capacity);
 
+/* VASP wave-coefficient export (src/half_vaspwave.F90:94-154): each k
+ * point's eigenvectors in VASP's plane-wave order (the box's x-fastest order,
+ * vasp_permutation :143-154) as interleaved single precision, band-major:
+ * packed[offsets[ik] + 2 * (ib * npws[ik] + ig) + {0, 1}] = (re, im), the
+ * layout of /wave/spin_1/kpoint_<k>/wave [nb][npw][2] in vaspwave.h5 (the
+ * HDF5 container itself is written by the caller's HDF5 library, as the
+ * reference's src/half_hdf5_bridge.c does).
+ * vectors: nk blocks of ld x nbands (column-major), host or device memory;
+ * packed: host or device memory of capacity floats (>= 2 * nbands *
+ * sum npw_k, else HALF_ERROR_CAPACITY), or NULL to query npws and offsets
+ * only.  npws[nk] and offsets[nk] (in floats) are always written. */
+int half_pack_vasp_waves(half_handle handle, int nk, const double *kpoints,
+                         int nbands, int64_t ld, const HALF_C128 *vectors,
+                         float *packed, int64_t capacity, int *npws,
+                         int64_t *offsets, char *error, int error_capacity);
+
 #ifdef __cplusplus
 }
 #endif

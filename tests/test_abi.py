@@ -27,7 +27,7 @@ def declared_symbols():
 def test_library_exports_every_declared_symbol():
     lib = halfb200.load_library()
     syms = declared_symbols()
-    assert len(syms) == 29
+    assert len(syms) == 30
     for s in syms:
         assert hasattr(lib, s), s
     out = subprocess.run(["nm", "-D", "--defined-only", halfb200.library_path()], capture_output=True, text=True).stdout
