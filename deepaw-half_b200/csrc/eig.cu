@@ -492,222 +492,149 @@ __global__ void __launch_bounds__(kFactorThreads) metric_factor_kernel(double2* 
   if (tid == 0) *status = s_bad;
 }
 
+// Block-wide sum of a (real, imaginary) pair; every thread gets the result.
+__device__ double2 block_sum2(double a, double b, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, off);
+    b += __shfl_xor_sync(0xffffffffu, b, off);
+  }
+  __syncthreads();   // red may still be read by a previous call
+  if (lane == 0) { red[2 * warp] = a; red[2 * warp + 1] = b; }
+  __syncthreads();
+  double sa = 0, sb = 0;
+  for (int w = 0; w < nw; ++w) { sa += red[2 * w]; sb += red[2 * w + 1]; }
+  return make_double2(sa, sb);
+}
+
 // Householder reduction of a Hermitian A (n x n, upper triangle read) to the
 // real tridiagonal T = Q^H A Q, in the storage convention of LAPACK zhetrd
 // with UPLO = 'U' (the published zhetd2 algorithm): for i = n-2 .. 0 the
 // reflector H(i) = I - tau_i v v^H with v(i) = 1 and v(0:i-1) left in
 // A(0:i-1, i+1) annihilates A(0:i-1, i+1); d = diag(T), e = superdiagonal.
-// Per step: x = tau A v (Hermitian), alpha = -tau (x^H v) / 2,
-// w = x + alpha v, A -= v w^H + w v^H (the diagonal kept real, as zher2 does).
-//
-// One CTA with the packed upper triangle in shared memory (n <= kTrdMax).
-// Each stored element is read once per matrix-vector product: warp w takes
-// columns s = w, w + 16, ...; its lanes own rows r = lane + 32 t and keep v_r,
-// w_r and their share of (U v)_r in registers, while the column dot
-// (U^H v)_s is a warp reduction.  The per-warp row partials are summed in a
-// fixed order, so the result does not depend on scheduling.  The column the
-// next step reflects is the last one this step updates; its warp computes
-// the next norm on the fly, and every thread evaluates zlarfg itself, so a
-// step takes four CTA barriers.
-constexpr int kTrdThreads = 512;
-constexpr int kTrdWarps = kTrdThreads / 32;
-constexpr int kTrdMax = 148;                     // packed triangle + 19 n-vectors within kSmemMax
-constexpr int kTrdRows = (kTrdMax + 31) / 32;    // lane-owned rows per thread
-
-__device__ __forceinline__ double2 cmul_(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cmulc_(double2 a, double2 b) {   // conj(a) b
-  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
-}
-
-__global__ void __launch_bounds__(kTrdThreads) hetrd_kernel(double2* __restrict__ A, int n, double* __restrict__ dout,
-                                                           double* __restrict__ eout, double2* __restrict__ tauout) {
+// One CTA; the packed upper triangle stays in shared memory for the whole
+// reduction (n <= kMetricMax), replacing a launch pair per reflector.
+__global__ void __launch_bounds__(512) hetrd_kernel(double2* __restrict__ A, int n, double* __restrict__ dout,
+                                                    double* __restrict__ eout, double2* __restrict__ tauout) {
   extern __shared__ double2 pk[];
-  double2* v = pk + size_t(n) * (n + 1) / 2;   // reflector
-  double2* y = v + n;                          // tau A v
-  double2* dcol = y + n;                       // (U^H v)_s, strictly upper part
-  double2* part = dcol + n;                    // [warp][row] partial (U v)_r
-  __shared__ double red[2 * kTrdWarps];
-  __shared__ double s_xn2;
-  __shared__ double2 s_alpha;
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5, lane = tid & 31;
+  double2* v = pk + size_t(n) * (n + 1) / 2;
+  double2* y = v + n;
+  __shared__ double red[64];
+  __shared__ double2 s_tau, s_scale, s_alpha2;
+  __shared__ double s_beta;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
   auto at = [](int i, int j) { return j * (j + 1) / 2 + i; };
-  for (int j = warp; j < n; j += kTrdWarps) {
-    double2* col = pk + j * (j + 1) / 2;
-    for (int i = lane; i <= j; i += 32) {
-      double2 a = A[size_t(j) * n + i];
+  for (int q = tid; q < n * n; q += nt) {
+    const int i = q % n, j = q / n;
+    if (i <= j) {
+      double2 a = A[q];
       if (i == j) a.y = 0.0;
-      col[i] = a;
+      pk[at(i, j)] = a;
     }
   }
-  __syncthreads();
-  // norm and alpha of the first reflected column (c = n-1): rows 0..n-3, A(n-2, n-1)
-  auto column_norm = [&](int c) {   // one warp; c >= 1
-    const double2* col = pk + c * (c + 1) / 2;
-    double x2 = 0;
-    for (int r = lane; r < c - 1; r += 32) x2 += col[r].x * col[r].x + col[r].y * col[r].y;
-    for (int off = 16; off > 0; off >>= 1) x2 += __shfl_xor_sync(0xffffffffu, x2, off);
-    if (lane == 0) {
-      s_xn2 = x2;
-      s_alpha = col[c - 1];
-    }
-  };
-  if (n >= 2 && warp == 0) column_norm(n - 1);
   __syncthreads();
   for (int i0 = n - 2; i0 >= 0; --i0) {
     const int L = i0 + 1, c = i0 + 1;
-    // zlarfg on (alpha = A(i0, c), x = A(0:i0-1, c)), evaluated by every thread
-    const double xn2 = s_xn2;
-    const double2 al = s_alpha;
-    double2 tau, sc;
-    double beta;
-    if (xn2 == 0.0 && al.y == 0.0) {
-      tau = make_double2(0.0, 0.0);
-      beta = al.x;
-      sc = make_double2(1.0, 0.0);
-    } else {
-      beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
-      tau = make_double2((beta - al.x) / beta, -al.y / beta);
-      const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
-      sc = make_double2(dr / den, -di / den);   // 1 / (alpha - beta)
+    // zlarfg on (alpha = A(i0, c), x = A(0:i0-1, c))
+    double part = 0;
+    for (int r = tid; r < i0; r += nt) {
+      const double2 x = pk[at(r, c)];
+      part += x.x * x.x + x.y * x.y;
     }
-    double2* colc = pk + c * (c + 1) / 2;
-    for (int r = tid; r < L; r += kTrdThreads) {
+    const double xn2 = block_sum2(part, 0.0, red).x;
+    if (tid == 0) {
+      const double2 al = pk[at(i0, c)];
+      if (xn2 == 0.0 && al.y == 0.0) {
+        s_tau = make_double2(0.0, 0.0);
+        s_beta = al.x;
+        s_scale = make_double2(1.0, 0.0);
+      } else {
+        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double dr = al.x - beta, di = al.y, den = dr * dr + di * di;
+        s_scale = make_double2(dr / den, -di / den);   // 1 / (alpha - beta)
+        s_beta = beta;
+      }
+    }
+    __syncthreads();
+    const double2 tau = s_tau, sc = s_scale;
+    for (int r = tid; r < L; r += nt) {
       double2 vr = make_double2(1.0, 0.0);
       if (r < i0) {
-        vr = cmul_(colc[r], sc);
-        colc[r] = vr;
+        const double2 x = pk[at(r, c)];
+        vr = make_double2(x.x * sc.x - x.y * sc.y, x.x * sc.y + x.y * sc.x);
+        pk[at(r, c)] = vr;
       }
       v[r] = vr;
     }
-    if (tid == 0) {
-      eout[i0] = beta;
-      tauout[i0] = tau;
-      dout[c] = pk[at(c, c)].x;   // final: later steps touch rows and columns 0..i0 only
-    }
     __syncthreads();
-    if (tau.x == 0.0 && tau.y == 0.0) {   // H = I: nothing to update
-      if (i0 >= 1 && warp == 0) column_norm(i0);
-      __syncthreads();
-      continue;
-    }
-    double2 vr[kTrdRows], acc[kTrdRows];
-#pragma unroll
-    for (int t = 0; t < kTrdRows; ++t) {
-      const int r = lane + 32 * t;
-      vr[t] = r < L ? v[r] : make_double2(0.0, 0.0);
-      acc[t] = make_double2(0.0, 0.0);
-    }
-    // matrix-vector product: column s contributes A(r,s) v_s to rows r <= s
-    // and conj(A(r,s)) v_r (r < s) to row s
-    for (int s2 = warp; s2 < L; s2 += kTrdWarps) {
-      const double2 vs = v[s2];
-      const double2* cs = pk + s2 * (s2 + 1) / 2;
-      double dr = 0, di = 0;
-#pragma unroll
-      for (int t = 0; t < kTrdRows; ++t) {
-        const int r = lane + 32 * t;
-        if (r <= s2) {
-          const double2 a = cs[r];
-          const double2 p = cmul_(a, vs);
-          acc[t].x += p.x;
-          acc[t].y += p.y;
-          if (r < s2) {
-            const double2 q = cmulc_(a, vr[t]);
-            dr += q.x;
-            di += q.y;
+    if (tau.x != 0.0 || tau.y != 0.0) {
+      // y = tau A(0:i0, 0:i0) v: g = 2^k threads per row, partial sums over
+      // s = p, p + g, ... combined by shuffles (deterministic order)
+      {
+        int lg = 0;
+        while (lg < 5 && (2 << lg) * L <= nt) ++lg;
+        const int g = 1 << lg, r = tid >> lg, p = tid & (g - 1);
+        double sr = 0, si = 0;
+        if (r < L) {
+          const double2* cr = pk + r * (r + 1) / 2;   // column r: A(s, r), s <= r
+          for (int s2 = p; s2 < L; s2 += g) {
+            double2 a;
+            if (r <= s2) a = pk[s2 * (s2 + 1) / 2 + r];
+            else { a = cr[s2]; a.y = -a.y; }
+            const double2 vv = v[s2];
+            sr += a.x * vv.x - a.y * vv.y;
+            si += a.x * vv.y + a.y * vv.x;
           }
         }
+        for (int off = g >> 1; off > 0; off >>= 1) {
+          sr += __shfl_xor_sync(0xffffffffu, sr, off);
+          si += __shfl_xor_sync(0xffffffffu, si, off);
+        }
+        if (r < L && p == 0) y[r] = make_double2(tau.x * sr - tau.y * si, tau.x * si + tau.y * sr);
       }
-      for (int off = 16; off > 0; off >>= 1) {
-        dr += __shfl_xor_sync(0xffffffffu, dr, off);
-        di += __shfl_xor_sync(0xffffffffu, di, off);
+      __syncthreads();
+      // alpha2 = -tau (y^H v) / 2; w = y + alpha2 v
+      double pr = 0, pi = 0;
+      for (int r = tid; r < L; r += nt) {
+        const double2 yy = y[r], vv = v[r];
+        pr += yy.x * vv.x + yy.y * vv.y;   // conj(y) v
+        pi += yy.x * vv.y - yy.y * vv.x;
       }
-      if (lane == 0) dcol[s2] = make_double2(dr, di);
-    }
-#pragma unroll
-    for (int t = 0; t < kTrdRows; ++t) {
-      const int r = lane + 32 * t;
-      if (r < L) part[warp * n + r] = acc[t];
-    }
-    __syncthreads();
-    // y = tau (U v + U^H v), and the partial of y^H v
-    double pr = 0, pi = 0;
-    for (int r = tid; r < L; r += kTrdThreads) {
-      double2 sum = dcol[r];
-      for (int w = 0; w < kTrdWarps; ++w) {
-        const double2 q = part[w * n + r];
-        sum.x += q.x;
-        sum.y += q.y;
+      const double2 dot = block_sum2(pr, pi, red);
+      if (tid == 0) s_alpha2 = make_double2(-0.5 * (tau.x * dot.x - tau.y * dot.y), -0.5 * (tau.x * dot.y + tau.y * dot.x));
+      __syncthreads();
+      const double2 a2 = s_alpha2;
+      for (int r = tid; r < L; r += nt) {
+        const double2 vv = v[r];
+        y[r].x += a2.x * vv.x - a2.y * vv.y;
+        y[r].y += a2.x * vv.y + a2.y * vv.x;
       }
-      const double2 yr = cmul_(tau, sum);
-      y[r] = yr;
-      const double2 q = cmulc_(yr, v[r]);
-      pr += q.x;
-      pi += q.y;
-    }
-    for (int off = 16; off > 0; off >>= 1) {
-      pr += __shfl_xor_sync(0xffffffffu, pr, off);
-      pi += __shfl_xor_sync(0xffffffffu, pi, off);
-    }
-    if (lane == 0) {
-      red[2 * warp] = pr;
-      red[2 * warp + 1] = pi;
-    }
-    __syncthreads();
-    // alpha = -tau (y^H v) / 2 (every thread, fixed order); w = y + alpha v
-    double2 dot = make_double2(0.0, 0.0);
-    for (int w = 0; w < kTrdWarps; ++w) {
-      dot.x += red[2 * w];
-      dot.y += red[2 * w + 1];
-    }
-    const double2 td = cmul_(tau, dot);
-    const double2 a2 = make_double2(-0.5 * td.x, -0.5 * td.y);
-    double2 wr[kTrdRows];
-#pragma unroll
-    for (int t = 0; t < kTrdRows; ++t) {
-      const int r = lane + 32 * t;
-      if (r < L) {
-        const double2 q = cmul_(a2, vr[t]), yy = y[r];
-        wr[t] = make_double2(yy.x + q.x, yy.y + q.y);
-      } else {
-        wr[t] = make_double2(0.0, 0.0);
-      }
-    }
-    // A(0:i0, 0:i0) -= v w^H + w v^H; the warp of column i0 (reflected next)
-    // also forms its norm over rows 0..i0-2 and alpha = A(i0-1, i0)
-    for (int s2 = warp; s2 < L; s2 += kTrdWarps) {
-      const double2 vs = v[s2], yy = y[s2], q0 = cmul_(a2, vs);
-      const double2 ws = make_double2(yy.x + q0.x, yy.y + q0.y);
-      double2* cs = pk + s2 * (s2 + 1) / 2;
-      double x2 = 0;
-#pragma unroll
-      for (int t = 0; t < kTrdRows; ++t) {
-        const int r = lane + 32 * t;
-        if (r <= s2) {
-          double2 a = cs[r];
-          // v_r conj(w_s) + w_r conj(v_s)
-          a.x -= (vr[t].x * ws.x + vr[t].y * ws.y) + (wr[t].x * vs.x + wr[t].y * vs.y);
-          a.y -= (vr[t].y * ws.x - vr[t].x * ws.y) + (wr[t].y * vs.x - wr[t].x * vs.y);
-          if (r == s2) a.y = 0.0;
-          cs[r] = a;
-          if (r < s2 - 1) x2 += a.x * a.x + a.y * a.y;
-          if (s2 == i0 && r == s2 - 1) s_alpha = a;
+      __syncthreads();
+      // A(0:i0, 0:i0) -= v w^H + w v^H (upper triangle), one warp per column
+      for (int s2 = warp; s2 < L; s2 += nw) {
+        const double2 ws = y[s2], vs = v[s2];
+        double2* cs = pk + s2 * (s2 + 1) / 2;
+        for (int r = lane; r <= s2; r += 32) {
+          const double2 vr = v[r], wr = y[r];
+          cs[r].x -= (vr.x * ws.x + vr.y * ws.y) + (wr.x * vs.x + wr.y * vs.y);
+          cs[r].y -= (vr.y * ws.x - vr.x * ws.y) + (wr.y * vs.x - wr.x * vs.y);
         }
       }
-      if (s2 == i0 && i0 >= 1) {
-        for (int off = 16; off > 0; off >>= 1) x2 += __shfl_xor_sync(0xffffffffu, x2, off);
-        if (lane == 0) s_xn2 = x2;
-      }
+      __syncthreads();
     }
-    __syncthreads();
+    if (tid == 0) {
+      eout[i0] = s_beta;
+      dout[i0 + 1] = pk[at(i0 + 1, i0 + 1)].x;
+      tauout[i0] = tau;
+    }
   }
-  if (tid == 0) dout[0] = pk[0].x;
-  for (int j = warp; j < n; j += kTrdWarps) {   // reflector vectors back to A (strict upper triangle)
-    const double2* col = pk + j * (j + 1) / 2;
-    for (int i = lane; i < j; i += 32) A[size_t(j) * n + i] = col[i];
+  __syncthreads();
+  if (tid == 0) dout[0] = pk[at(0, 0)].x;
+  for (int q = tid; q < n * n; q += nt) {   // reflector vectors back to A (strict upper triangle)
+    const int i = q % n, j = q / n;
+    if (i < j) A[q] = pk[at(i, j)];
   }
 }
 
@@ -743,10 +670,10 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
 void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* status) {
   reserve(rt, n);
   cudaStream_t s = rt.stream;
-  if (n <= kTrdMax) {   // whole reduction in one CTA
-    const size_t tsm = (size_t(n) * (n + 1) / 2 + (3 + size_t(kTrdWarps)) * n) * sizeof(double2);
+  if (n <= kMetricMax) {   // whole reduction in one CTA
+    const size_t tsm = (size_t(n) * (n + 1) / 2 + 2 * size_t(n)) * sizeof(double2);
     raise_smem_limit(hetrd_kernel, tsm);
-    hetrd_kernel<<<1, kTrdThreads, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
+    hetrd_kernel<<<1, 512, tsm, s>>>(A, n, d.get(), e.get(), tau.get());
     HALF_LAUNCH("Householder tridiagonalisation");
     rt.prof.launches += 1;
   } else {
