@@ -821,13 +821,14 @@ extern "C" int half_ionic_forces(half_handle handle, const double* output_densit
     return HALF_ERROR_INVALID_ARGUMENT;
   }
   return guarded(error, cap, [&]() -> int {
-    if (output_density)
+    const bool dens_dev = output_density && device_pointer(output_density);
+    if (output_density && !dens_dev)
       for (int64_t i = 0; i < n; ++i)
         if (!std::isfinite(output_density[i])) fail(kInvalidArgument, "output density must be finite");
     IonicForces f;
     ctx->last = SolveInfo();
     begin_call(*ctx->rt);
-    ionic_forces_device(*ctx, output_density, false, ewald || energies, local || energies, nlcc != nullptr,
+    ionic_forces_device(*ctx, output_density, dens_dev, ewald || energies, local || energies, nlcc != nullptr,
                         harris != nullptr, f);
     end_call(*ctx->rt, ctx->last);
     if (ewald) std::copy(f.ewald.begin(), f.ewald.end(), ewald);
@@ -860,6 +861,7 @@ extern "C" int half_output_density(half_handle handle, int nk, const double* kpo
     for (int ik = 0; ik < nk; ++ik)
       if (!finite3(kpoints + 3 * ik)) fail(kInvalidArgument, "k point must be finite");
     cudaStream_t st = ctx->rt->stream;
+    const bool vec_dev = device_pointer(vectors);   // device eigenvectors are read in place
     std::vector<DeviceBuffer<double2>> dv(nk);
     std::vector<const double2*> ptr(nk);
     std::vector<long long> lds(nk);
@@ -867,8 +869,13 @@ extern "C" int half_output_density(half_handle handle, int nk, const double* kpo
       const Basis b = build_basis(ctx->crystal, ctx->charge.shape, ctx->encut, kpoints + 3 * ik);
       const long long npw = b.npw();
       if (ld < npw) fail(kCapacity, "eigenvector leading dimension is too small");
+      const double2* src = reinterpret_cast<const double2*>(vectors) + (size_t)ik * ld * nbands;
+      if (vec_dev) {
+        ptr[ik] = src;
+        lds[ik] = ld;
+        continue;
+      }
       dv[ik].resize((size_t)npw * nbands);
-      const HALF_C128* src = vectors + (size_t)ik * ld * nbands;
       HALF_CUDA(cudaMemcpy2DAsync(dv[ik].get(), npw * sizeof(double2), src, ld * sizeof(double2),
                                   npw * sizeof(double2), nbands, cudaMemcpyHostToDevice, st));
       ptr[ik] = dv[ik].get();
@@ -880,7 +887,7 @@ extern "C" int half_output_density(half_handle handle, int nk, const double* kpo
     begin_call(*ctx->rt);
     output_density_device(*ctx, nk, kpoints, kweights, nbands, ptr, lds, occupations, out.get(), &aug);
     end_call(*ctx->rt, ctx->last);
-    HALF_CUDA(cudaMemcpyAsync(density, out.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaMemcpyAsync(density, out.get(), sizeof(double) * n, cudaMemcpyDefault, st));
     HALF_CUDA(cudaStreamSynchronize(st));
     if (augmentation_charge) *augmentation_charge = aug;
     return HALF_SUCCESS;

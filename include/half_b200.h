@@ -151,8 +151,9 @@ int half_band_forces(half_handle handle, int nk, const double *kpoints,
  *   harris  frozen-input Harris response from the context's density to the
  *           output density (:129-161); zero without a partial core.
  * output_density: n values on the context's grid in the CHGCAR convention
- * (x fastest, rho * Omega), normally the smooth plus augmentation density of
- * the solved states; NULL = the context's own density (Harris is then zero).
+ * (x fastest, rho * Omega), host or device memory, normally the smooth plus
+ * augmentation density of the solved states; NULL = the context's own
+ * density (Harris is then zero).
  * energies (NULL to skip) [6] = {Ewald total, real-space, reciprocal, self,
  * background (src/half_energy.F90:122-162), local ionic energy on the output
  * density}. */
@@ -166,10 +167,11 @@ int half_ionic_forces(half_handle handle, const double *output_density,
  * the MIMIC_US augmentation density of the occupancies
  * rho_ij = sum w f Re(conj(c_i) c_j), c = B^H psi (src/half_uspp.F90:26-111).
  * vectors: nk consecutive blocks of ld x nbands (column-major, ld >= npw of
- * every k point); occupations [nk][nbands] (bands with f = 0 contribute
- * nothing).  density: n values on the context's grid in the CHGCAR convention
- * (x fastest, rho * Omega), overwritten; n must equal the grid size, else
- * HALF_ERROR_CAPACITY.  augmentation_charge (NULL to skip): the augmentation's
+ * every k point), host or device memory (device blocks are read in place);
+ * occupations [nk][nbands] (bands with f = 0 contribute nothing).  density:
+ * n values on the context's grid in the CHGCAR convention (x fastest,
+ * rho * Omega), host or device memory, overwritten; n must equal the grid
+ * size, else HALF_ERROR_CAPACITY.  augmentation_charge (NULL to skip): the augmentation's
  * contribution to the grid average, the reference's integrated_charge. */
 int half_output_density(half_handle handle, int nk, const double *kpoints,
                         const double *kweights, int nbands, int64_t ld,

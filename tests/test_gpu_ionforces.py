@@ -171,3 +171,43 @@ def test_forces_rejects_an_occupied_top_band(si2c):
     with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="evd") as ctx:
         with pytest.raises(halfb200.HalfError):
             ctx.forces(KPTS, WTS, 4, 8.0, 0.1, -1)
+
+
+def test_device_buffers_give_the_host_results(si2c):
+    """half_output_density and half_ionic_forces read device eigenvectors and a device
+    density in place; the results are the host-buffer results bit for bit."""
+    import ctypes as C
+    import torch
+    from oracle import hamiltonian as H
+    w, ch, po = si2c
+    sysm = load(si2c)
+    nb = 6
+    vecs = [H.solve_dense(H.prepare(sysm, k), nb, vectors=True)[1] for k in KPTS]
+    occ = np.array([[2.0, 2.0, 2.0, 1.0, 0.5, 0.0], [2.0, 2.0, 1.5, 1.5, 0.5, 0.0]])
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
+        host_rho, host_q = ctx.output_density(KPTS, WTS, vecs, occ)
+        ld = max(v.shape[0] for v in vecs)
+        block = np.zeros((len(KPTS), nb, ld), dtype=np.complex128)
+        for ik, v in enumerate(vecs):
+            block[ik, :, :v.shape[0]] = v.T
+        dvec = torch.from_numpy(block.view(np.float64).copy()).cuda()
+        drho = torch.zeros(host_rho.size, dtype=torch.float64, device="cuda")
+        ks = np.ascontiguousarray(np.asarray(KPTS, dtype=np.float64))
+        ws = np.ascontiguousarray(np.asarray(WTS, dtype=np.float64))
+        oc = np.ascontiguousarray(occ)
+        q = C.c_double(0.0)
+        err = C.create_string_buffer(256)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        st = ctx.lib.half_output_density(ctx.handle, len(KPTS), p(ks), p(ws), nb, ld, C.c_void_p(dvec.data_ptr()),
+                                         p(oc), C.c_void_p(drho.data_ptr()), host_rho.size, C.byref(q), err, 256)
+        assert st == halfb200.HALF_SUCCESS, err.value
+        torch.cuda.synchronize()
+        assert np.array_equal(drho.cpu().numpy(), host_rho) and q.value == host_q
+        host_f = ctx.ionic_forces(host_rho)
+        outs = [np.zeros((ctx.nions, 3)) for _ in range(4)]
+        en = np.zeros(6)
+        st = ctx.lib.half_ionic_forces(ctx.handle, C.c_void_p(drho.data_ptr()), host_rho.size, *[p(o) for o in outs],
+                                       p(en), err, 256)
+        assert st == halfb200.HALF_SUCCESS, err.value
+        for o, key in zip(outs, ("ewald", "local", "nlcc", "harris")):
+            assert np.array_equal(o, host_f[key]), key
