@@ -114,14 +114,18 @@ __global__ void residual_norm_kernel(const C* __restrict__ hx, const C* __restri
 
 // P = -R / (|T - eps| + 1), or the unit seed (m + j) mod n for bands whose
 // residual norm is below the seed threshold (src/half_cuda_iterative_solver.cuf:42-64, 150-155)
+// Output column a takes band cols[a] (cols null: band a), a < np.
 template <typename C>
 __global__ void precondition_kernel(const C* __restrict__ hx, const C* __restrict__ sx, long long ld, int n, int m,
-                                    const double* __restrict__ eps, const double* __restrict__ norms,
-                                    double seed_threshold, const double* __restrict__ kinetic, C* __restrict__ p) {
+                                    int np, const int* __restrict__ cols, const double* __restrict__ eps,
+                                    const double* __restrict__ norms, double seed_threshold,
+                                    const double* __restrict__ kinetic, C* __restrict__ p) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)n * m) return;
-  int j = int(t / n), i = int(t - (long long)j * n);
+  if (t >= (long long)n * np) return;
+  const int a = int(t / n), i = int(t - (long long)a * n);
+  const int j = cols ? cols[a] : a;
   long long o = (long long)j * ld + i;
+  const long long oa = (long long)a * ld + i;
   C out;
   if (norms[j] < seed_threshold) {
     int seed = (m + j) % n;
@@ -133,7 +137,7 @@ __global__ void precondition_kernel(const C* __restrict__ hx, const C* __restric
     out.x = -(double(hx[o].x) - e * double(sx[o].x)) / den;
     out.y = -(double(hx[o].y) - e * double(sx[o].y)) / den;
   }
-  p[o] = out;
+  p[oa] = out;
 }
 
 // U[:, j] /= sqrt(max(mu_j, floor))  (src/half_cuda_iterative_solver.cuf:66-77)
@@ -286,20 +290,22 @@ struct Blocks {
 struct Scratch64 {
   DeviceBuffer<double2> metric, hsub, ssub;   // m x m, 2m x 2m, 2m x 2m
   DeviceBuffer<double> w, mu, norms, kinetic;
-  DeviceBuffer<int> idx;
+  DeviceBuffer<int> idx, active;
 };
 
-// projected blocks into a (2m x 2m, ld 2m) FP64 matrix: [0:m,0:m]=A^H B1,
-// [0:m,m:2m]=A^H B2, [m:2m,m:2m]=P^H B2 (upper triangle is what zhegvd reads)
+// projected blocks into an ((m + np) x (m + np), ld m + np) FP64 matrix:
+// [0:m,0:m] = A^H B1, [0:m,m:] = A^H B2, [m:,m:] = P^H B2 (the upper triangle
+// is what zhegvd reads); np = m is the reference's 2m x 2m pencil.
 template <typename R>
-void project_upper(Runtime& rt, int n, int m, const cplx_t<R>* x, const cplx_t<R>* p, const cplx_t<R>* bx,
+void project_upper(Runtime& rt, int n, int m, int np, const cplx_t<R>* x, const cplx_t<R>* p, const cplx_t<R>* bx,
                    const cplx_t<R>* bp, cplx_t<R>* tmp2m, double2* out) {
   const auto one = cval<R>(1.0), zero = cval<R>(0.0);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, x, n, bx, n, zero, tmp2m, 2 * m);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, x, n, bp, n, zero, tmp2m + (long long)m * 2 * m, 2 * m);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, p, n, bp, n, zero, tmp2m + (long long)m * 2 * m + m, 2 * m);
+  const int ld = m + np;
+  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, x, n, bx, n, zero, tmp2m, ld);
+  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, one, x, n, bp, n, zero, tmp2m + (long long)m * ld, ld);
+  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, p, n, bp, n, zero, tmp2m + (long long)m * ld + m, ld);
   if constexpr (sizeof(R) == 4) {
-    long long tot = 4LL * m * m;
+    long long tot = (long long)ld * ld;
     convert_kernel<float2, double2><<<ceil_div(tot, 256), 256, 0, rt.stream>>>(tmp2m, out, tot);
     ++rt.prof.launches;
   }
@@ -387,23 +393,31 @@ struct AccRun {
     return mx;
   }
 
-  // one ACC iteration after the residual check (src/half_cuda_iterative_solver.cuf:158-195)
-  void iterate(double seed_threshold) {
+  // one ACC iteration after the residual check (src/half_cuda_iterative_solver.cuf:158-195).
+  // active (guard-band modes only; null = every band, the reference's step):
+  // the bands whose correction directions enter P, in order.
+  void iterate(double seed_threshold, const std::vector<int>* active = nullptr) {
     const auto one = cval<R>(1.0), zero = cval<R>(0.0), mone = cval<R>(-1.0);
-    long long nm = (long long)n * m;
-    precondition_kernel<C><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(blk.hx(), blk.sx(), n, n, m, sc.w.get(),
+    const int np = active ? int(active->size()) : m;
+    const int* cols = nullptr;
+    if (np < m) {
+      sc.active.upload(*active, rt.stream);
+      cols = sc.active.get();
+    }
+    long long nm = (long long)n * np;
+    precondition_kernel<C><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(blk.hx(), blk.sx(), n, n, m, np, cols, sc.w.get(),
                                                                        sc.norms.get(), seed_threshold, sc.kinetic.get(),
                                                                        blk.P.get());
     ++rt.prof.launches;
     HALF_LAUNCH("precondition");
     mark("precondition");
-    apply(blk.P.get(), blk.HP.get(), blk.SP.get(), m);
+    apply(blk.P.get(), blk.HP.get(), blk.SP.get(), np);
     mark("apply");
     // S-orthogonalise against X
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.SP.get(), n, zero, blk.small.get(), m);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.x(), n, blk.small.get(), m, one, blk.P.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.hx(), n, blk.small.get(), m, one, blk.HP.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, mone, blk.sx(), n, blk.small.get(), m, one, blk.SP.get(), n);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, one, blk.x(), n, blk.SP.get(), n, zero, blk.small.get(), m);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, blk.x(), n, blk.small.get(), m, one, blk.P.get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, blk.hx(), n, blk.small.get(), m, one, blk.HP.get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, blk.sx(), n, blk.small.get(), m, one, blk.SP.get(), n);
     mark("orth_gemm");
     // In the guard-band modes, when the library's own pencil solver takes
     // the Rayleigh-Ritz step, the separate S-metric normalisation is
@@ -411,61 +425,62 @@ struct AccRun {
     // pivots exactly like the metric step, so [X P] spans the same space
     // and the Ritz pairs are the same.  The FP64 mode keeps the reference's
     // metric step.
-    const bool skip_metric = guarded && ss.own && 2 * m <= SmallEigen::kOwnMaxOrder;
+    const int ord = m + np;
+    const bool skip_metric = guarded && ss.own && ord <= SmallEigen::kOwnMaxOrder;
     C* pu = skip_metric ? blk.P.get() : blk.PU.get();
     C* hpu = skip_metric ? blk.HP.get() : blk.HPU.get();
     C* spu = skip_metric ? blk.SP.get() : blk.SPU.get();
-    if (!skip_metric) normalise_metric(one, zero);
+    if (!skip_metric) normalise_metric(one, zero, np);
     // Rayleigh-Ritz on Z = [X PU]
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
     if constexpr (sizeof(R) == 8) {
-      project_upper<R>(rt, n, m, blk.x(), pu, blk.hx(), hpu, hs, hs);
-      project_upper<R>(rt, n, m, blk.x(), pu, blk.sx(), spu, ssb, ssb);
+      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs, hs);
+      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb, ssb);
     } else {
-      project_upper<R>(rt, n, m, blk.x(), pu, blk.hx(), hpu, tmp2m.get(), hs);
-      project_upper<R>(rt, n, m, blk.x(), pu, blk.sx(), spu, tmp2m.get(), ssb);
+      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, tmp2m.get(), hs);
+      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, tmp2m.get(), ssb);
     }
     mark("rr_gemm");
-    ss.hegvd(hs, ssb, 2 * m, sc.w.get(), m);
+    ss.hegvd(hs, ssb, ord, sc.w.get(), m);
     mark("hegvd");
-    to_r(hs, 2 * m, blk.Y.get(), 2 * m, 2 * m, m);
+    to_r(hs, ord, blk.Y.get(), ord, ord, m);
     const C* ytop = blk.Y.get();
     const C* ybot = blk.Y.get() + m;
     int nx = blk.cur ^ 1;
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, ytop, 2 * m, zero, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, pu, n, ybot, 2 * m, one, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.hx(), n, ytop, 2 * m, zero, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, hpu, n, ybot, 2 * m, one, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, 2 * m, zero, blk.SX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, spu, n, ybot, 2 * m, one, blk.SX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, ytop, ord, zero, blk.X[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, pu, n, ybot, ord, one, blk.X[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.hx(), n, ytop, ord, zero, blk.HX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, hpu, n, ybot, ord, one, blk.HX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, ord, zero, blk.SX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, spu, n, ybot, ord, one, blk.SX[nx].get(), n);
     blk.cur = nx;
     mark("rr_rot");
   }
 
-  // S-metric normalisation of P, HP, SP into PU, HPU, SPU
+  // S-metric normalisation of the np columns of P, HP, SP into PU, HPU, SPU
   // (src/half_cuda_iterative_solver.cuf:166-176)
-  void normalise_metric(cplx_t<R> one, cplx_t<R> zero) {
+  void normalise_metric(cplx_t<R> one, cplx_t<R> zero, int np) {
     double2* metric = sc.metric.get();
     if constexpr (sizeof(R) == 8) {
-      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.P.get(), n, blk.SP.get(), n, zero, metric, m);
+      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, blk.P.get(), n, blk.SP.get(), n, zero, metric, np);
     } else {
-      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.P.get(), n, blk.SP.get(), n, zero, blk.small.get(), m);
-      convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(blk.small.get(), metric,
-                                                                                               (long long)m * m);
+      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, blk.P.get(), n, blk.SP.get(), n, zero, blk.small.get(), np);
+      convert_kernel<float2, double2><<<ceil_div((long long)np * np, 256), 256, 0, rt.stream>>>(blk.small.get(), metric,
+                                                                                                 (long long)np * np);
       ++rt.prof.launches;
     }
     mark("metric_gemm");
-    if (!(ss.own && ss.eig.metric_normalize(rt, metric, m, ss.info.get()))) {
-      ss.heevd(metric, m, sc.mu.get());
-      scale_columns_kernel<<<ceil_div(m * m, 256), 256, 0, rt.stream>>>(metric, m, sc.mu.get(), 1.0e-14);
+    if (!(ss.own && ss.eig.metric_normalize(rt, metric, np, ss.info.get()))) {
+      ss.heevd(metric, np, sc.mu.get());
+      scale_columns_kernel<<<ceil_div(np * np, 256), 256, 0, rt.stream>>>(metric, np, sc.mu.get(), 1.0e-14);
       ++rt.prof.launches;
     }
     mark("heevd");
-    to_r(metric, m, blk.small.get(), m, m, m);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.P.get(), n, blk.small.get(), m, zero, blk.PU.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.HP.get(), n, blk.small.get(), m, zero, blk.HPU.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.SP.get(), n, blk.small.get(), m, zero, blk.SPU.get(), n);
+    to_r(metric, np, blk.small.get(), np, np, np);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, np, one, blk.P.get(), n, blk.small.get(), np, zero, blk.PU.get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, np, one, blk.HP.get(), n, blk.small.get(), np, zero, blk.HPU.get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, np, one, blk.SP.get(), n, blk.small.get(), np, zero, blk.SPU.get(), n);
     mark("metric_rot");
   }
 };
@@ -505,6 +520,24 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   SmallSolver ss(rt, m, sc.hsub.get(), sc.ssub.get(), sc.w.get());
   const double seed_threshold = std::max(cfg.tol * 1e-2, 1e-12);
   std::vector<double> norms;
+  // Soft locking (guard-band modes): a requested band whose residual is at or
+  // below half the phase's tolerance keeps its Ritz vector in X but adds no
+  // correction direction to P, so late iterations solve pencils of order
+  // m + (active bands) instead of 2m and apply the operator to fewer columns.
+  // The set is recomputed every iteration (a band whose residual rises is
+  // active again); guard bands are always active.  Opt-in: HALF_SOFT_LOCK=1
+  // (guard-band modes only).  Without it every iteration takes the full 2m
+  // pencil, and the FP64 mode, the reference's iteration, never locks.
+  bool soft_lock = false;
+  if (const char* sl = std::getenv("HALF_SOFT_LOCK")) soft_lock = guarded && std::string(sl) == "1";
+  std::vector<int> active;
+  auto pick_active = [&](double lock_tol) -> const std::vector<int>* {
+    if (!soft_lock) return nullptr;
+    active.clear();
+    for (int j = 0; j < m; ++j)
+      if (j >= mreq || !(norms[j] <= lock_tol)) active.push_back(j);
+    return &active;
+  };
   int infos[3] = {0, 0, 0};
   int iter = 0, fp64_iter = 0;
   bool converged = false;
@@ -544,7 +577,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
       tracer.step("fp32", iter, max_res, norms);
       if (max_res < 0.9 * best) { best = max_res; since_best = 0; } else { ++since_best; }
       if (max_res <= switch_tol || since_best >= 6) break;
-      run32.iterate(seed_threshold);
+      run32.iterate(seed_threshold, pick_active(0.5 * switch_tol));
     }
     if (iter > cfg.max_iter) iter = cfg.max_iter;
     op_ms += run32.op_ms;
@@ -558,7 +591,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
       max_res = run64.residuals(norms, infos);
       tracer.step("fp64", fp64_iter, max_res, norms);
       if (max_res <= cfg.tol) { converged = true; break; }
-      run64.iterate(seed_threshold);
+      run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
     }
     fp64_iter = std::min(fp64_iter, cfg.max_iter);
     iter += fp64_iter;
@@ -571,7 +604,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
       max_res = run64.residuals(norms, infos);
       tracer.step("fp64", iter, max_res, norms);
       if (max_res <= cfg.tol) { converged = true; break; }
-      run64.iterate(seed_threshold);
+      run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
     }
     iter = std::min(iter, cfg.max_iter);
     fp64_iter = iter;
