@@ -150,3 +150,20 @@ def test_reference_c_api_test_passes_unchanged(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+
+
+def test_force_and_export_entries_reject_a_stale_handle():
+    """The additive force, density and export entries follow the ABI's handle
+    convention before reading any other argument (src/half_c_api.F90:636-640)."""
+    lib = halfb200.load_library()
+    err = C.create_string_buffer(128)
+    calls = [
+        lambda: lib.half_ionic_forces(12345, None, 0, None, None, None, None, None, err, 128),
+        lambda: lib.half_output_density(12345, 1, None, None, 1, 1, None, None, None, 0, None, err, 128),
+        lambda: lib.half_forces(12345, 1, None, None, 1, 8.0, 0.1, -1, None, None, None, None, err, 128),
+        lambda: lib.half_pack_vasp_waves(12345, 1, None, 1, 1, None, None, 0, None, None, err, 128),
+    ]
+    for call in calls:
+        err.value = b"stale"
+        assert call() == halfb200.HALF_ERROR_INVALID_HANDLE
+        assert err.value == b"invalid HALF context handle"
