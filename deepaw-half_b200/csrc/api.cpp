@@ -1016,3 +1016,27 @@ extern "C" int half_pack_vasp_waves(half_handle handle, int nk, const double* kp
     return HALF_SUCCESS;
   });
 }
+
+extern "C" int half_occupations(int nk, int nbands, const double* eigenvalues, const double* kweights, double nelect,
+                                double sigma, int ismear, double* occupations, double* energies, char* error,
+                                int cap) {
+  clear_error(error, cap);
+  if (nk < 1 || nbands < 1 || !eigenvalues || !kweights || !occupations) {
+    export_error("invalid occupation arguments", error, cap);
+    return HALF_ERROR_INVALID_ARGUMENT;
+  }
+  return guarded(error, cap, [&]() -> int {
+    for (long long i = 0; i < (long long)nk * nbands; ++i)
+      if (!std::isfinite(eigenvalues[i])) fail(kInvalidArgument, "eigenvalues must be finite");
+    std::vector<double> eig(eigenvalues, eigenvalues + (size_t)nk * nbands), occ;
+    double mu = 0, band = 0, entropy = 0;
+    compute_occupations(eig, nk, nbands, kweights, nelect, sigma, ismear, occ, mu, band, entropy);
+    std::copy(occ.begin(), occ.end(), occupations);
+    if (energies) {
+      energies[0] = band;
+      energies[1] = entropy;
+      energies[2] = mu;
+    }
+    return HALF_SUCCESS;
+  });
+}

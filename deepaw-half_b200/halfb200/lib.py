@@ -94,6 +94,7 @@ _SIGS = {
                             + _ERR),
     "half_pack_vasp_waves": (C.c_int, [C.c_int64, C.c_int, _P, C.c_int, C.c_int64, _P, _P, C.c_int64, _P, _P]
                              + _ERR),
+    "half_occupations": (C.c_int, [C.c_int, C.c_int, _P, _P, C.c_double, C.c_double, C.c_int, _P, _P] + _ERR),
     "half_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P, _P]
                     + _ERR),
 }
@@ -136,6 +137,21 @@ def version_string():
 
 def capabilities():
     return load_library().half_get_capabilities()
+
+
+def occupations(eigenvalues, weights, nelect, sigma, ismear=-1):
+    """half_occupations: (occupations (nk, nb), band energy, entropy term, mu).
+    A host routine; needs no context or GPU."""
+    eig = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64))
+    if eig.ndim != 2:
+        raise ValueError("eigenvalues must be (nk, nbands)")
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+    occ = np.zeros_like(eig)
+    en = np.zeros(3)
+    err = C.create_string_buffer(512)
+    _check(load_library().half_occupations(eig.shape[0], eig.shape[1], _ptr(eig), _ptr(w), float(nelect),
+                                           float(sigma), int(ismear), _ptr(occ), _ptr(en), err, 512), err)
+    return occ, en[0], en[1], en[2]
 
 
 class Context:

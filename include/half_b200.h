@@ -215,6 +215,21 @@ int half_pack_vasp_waves(half_handle handle, int nk, const double *kpoints,
                          float *packed, int64_t capacity, int *npws,
                          int64_t *offsets, char *error, int error_capacity);
 
+/* Band occupations for nelect electrons, restating compute_occupations
+ * (src/half_energy.F90:41-120); a host routine that needs no context or GPU.
+ * eigenvalues [nk][nbands] in eV, kweights summing to one (else
+ * HALF_ERROR_INVALID_ARGUMENT), sigma >= 0: zero fills degenerate levels
+ * fractionally in ascending order, otherwise ismear -1 (Fermi-Dirac) or 0
+ * (Gaussian) with the chemical potential found by bisection.  occupations
+ * [nk][nbands] in 0..2 are written; energies (NULL to skip) [3] = {band
+ * energy, entropy term, chemical potential}.  The same routine sets the
+ * occupations inside half_band_forces and half_forces; callers that shard
+ * k points over processes use it on the gathered eigenvalues. */
+int half_occupations(int nk, int nbands, const double *eigenvalues,
+                     const double *kweights, double nelect, double sigma,
+                     int ismear, double *occupations, double *energies,
+                     char *error, int error_capacity);
+
 #ifdef __cplusplus
 }
 #endif

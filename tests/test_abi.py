@@ -7,6 +7,7 @@ import re
 import shutil
 import subprocess
 
+import numpy as np
 import pytest
 
 import halfb200
@@ -27,7 +28,7 @@ def declared_symbols():
 def test_library_exports_every_declared_symbol():
     lib = halfb200.load_library()
     syms = declared_symbols()
-    assert len(syms) == 30
+    assert len(syms) == 31
     for s in syms:
         assert hasattr(lib, s), s
     out = subprocess.run(["nm", "-D", "--defined-only", halfb200.library_path()], capture_output=True, text=True).stdout
@@ -167,3 +168,26 @@ def test_force_and_export_entries_reject_a_stale_handle():
         err.value = b"stale"
         assert call() == halfb200.HALF_ERROR_INVALID_HANDLE
         assert err.value == b"invalid HALF context handle"
+
+
+def test_occupations_match_the_oracle_and_known_answers():
+    """half_occupations (host routine, no GPU) against app/half_energy_check.F90:19-34
+    and the oracle restatement of src/half_energy.F90:41-120 on seeded spectra."""
+    from oracle.forces import compute_occupations
+    occ, band, ent, mu = halfb200.occupations([[0.0, 2.0], [1.0, 3.0]], [0.5, 0.5], 2.0, 0.0)
+    assert np.abs(occ - np.array([[2.0, 0.0], [2.0, 0.0]])).max() <= 1e-14
+    assert abs(mu - 1.0) <= 1e-14 and abs(band - 1.0) <= 1e-14 and abs(ent) <= 1e-14
+    r = np.random.default_rng(3)
+    for nk, nb, nelect, sigma, ismear in ((4, 12, 9.0, 0.1, -1), (3, 10, 7.5, 0.05, 0), (2, 8, 6.0, 0.0, -1)):
+        eig = np.sort(r.normal(0.0, 3.0, size=(nk, nb)), axis=1)
+        w = r.uniform(0.5, 1.0, size=nk)
+        w /= w.sum()
+        occ, band, ent, mu = halfb200.occupations(eig, w, nelect, sigma, ismear)
+        o2, mu2, band2, ent2 = compute_occupations(eig, w, nelect, sigma, ismear)
+        assert np.abs(occ - o2).max() <= 1e-12 and abs(band - band2) <= 1e-11
+        assert abs(ent - ent2) <= 1e-12 and abs(mu - mu2) <= 1e-11
+        assert abs((w[:, None] * occ).sum() - nelect) <= 1e-10
+    with pytest.raises(halfb200.HalfError):
+        halfb200.occupations([[0.0, 1.0]], [0.7], 2.0, 0.1)        # weights must sum to one
+    with pytest.raises(halfb200.HalfError):
+        halfb200.occupations([[0.0, 1.0]], [1.0], 5.0, 0.1)        # more electrons than bands hold

@@ -211,3 +211,19 @@ def test_device_buffers_give_the_host_results(si2c):
         assert st == halfb200.HALF_SUCCESS, err.value
         for o, key in zip(outs, ("ewald", "local", "nlcc", "harris")):
             assert np.array_equal(o, host_f[key]), key
+
+
+def test_sharded_forces_on_one_rank_is_half_forces(si2c):
+    """halfb200.shard.sharded_forces composes the per-k entry points (solve,
+    half_occupations, half_nonlocal_forces, half_output_density,
+    half_ionic_forces); on one rank it must give what half_forces gives in one
+    call, to 1e-10 of each quantity's size."""
+    from halfb200.shard import sharded_forces
+    w, ch, po = si2c
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="evd") as ctx:
+        a = ctx.forces(KPTS, WTS, 16, 8.0, 0.1, -1)
+        b = sharded_forces(ctx, KPTS, WTS, 16, 8.0, 0.1, -1)
+    for key in ("forces", "ewald", "local", "nonlocal", "nlcc", "harris", "output_density"):
+        assert np.abs(a[key] - b[key]).max() <= 1e-10 * max(1.0, np.abs(a[key]).max()), key
+    for key in ("band_energy", "entropy", "mu", "ewald_energy", "local_energy", "augmentation_charge"):
+        assert abs(a[key] - b[key]) <= 1e-10 * max(1.0, abs(a[key])), key
