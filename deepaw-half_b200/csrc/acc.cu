@@ -24,8 +24,9 @@
 //   metric; both bases span the same space, so the Rayleigh-Ritz step and
 //   the Ritz values are those of the reference up to rounding;
 // * precision MIXED runs the iterations on FP32 blocks (FP32 operator,
-//   BF16x9 tensor-core GEMMs when cuBLAS provides them, FP64 small
-//   eigensolves) until the residual reaches the FP32 regime, then promotes X
+//   split-bf16 tcgen05 GEMMs from tc_gemm.cu whose projected matrices land
+//   directly in FP64, FP64 small eigensolves) until the residual reaches the
+//   FP32 regime, then promotes X
 //   and finishes with FP64 iterations (one FP64 operator sweep re-creates
 //   H X and S X exactly before the first FP64 Rayleigh-Ritz); it carries
 //   m/8 (at least 4) guard bands and tests convergence on the requested m.
@@ -296,18 +297,21 @@ struct Scratch64 {
 // projected blocks into an ((m + np) x (m + np), ld m + np) FP64 matrix:
 // [0:m,0:m] = A^H B1, [0:m,m:] = A^H B2, [m:,m:] = P^H B2 (the upper triangle
 // is what zhegvd reads); np = m is the reference's 2m x 2m pencil.
+// (FP32 blocks: tensor-core products written straight into the FP64 pencil,
+// split-K partial sums reduced in FP64.)
 template <typename R>
 void project_upper(Runtime& rt, int n, int m, int np, const cplx_t<R>* x, const cplx_t<R>* p, const cplx_t<R>* bx,
-                   const cplx_t<R>* bp, cplx_t<R>* tmp2m, double2* out) {
-  const auto one = cval<R>(1.0), zero = cval<R>(0.0);
+                   const cplx_t<R>* bp, double2* out) {
   const int ld = m + np;
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, x, n, bx, n, zero, tmp2m, ld);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, one, x, n, bp, n, zero, tmp2m + (long long)m * ld, ld);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, p, n, bp, n, zero, tmp2m + (long long)m * ld + m, ld);
   if constexpr (sizeof(R) == 4) {
-    long long tot = (long long)ld * ld;
-    convert_kernel<float2, double2><<<ceil_div(tot, 256), 256, 0, rt.stream>>>(tmp2m, out, tot);
-    ++rt.prof.launches;
+    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, x, n, bx, n, out, ld);
+    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, x, n, bp, n, out + (long long)m * ld, ld);
+    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, p, n, bp, n, out + (long long)m * ld + m, ld);
+  } else {
+    const auto one = cval<R>(1.0), zero = cval<R>(0.0);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, x, n, bx, n, zero, out, ld);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, one, x, n, bp, n, zero, out + (long long)m * ld, ld);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, p, n, bp, n, zero, out + (long long)m * ld + m, ld);
   }
 }
 
@@ -358,12 +362,8 @@ struct AccRun {
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.hx(), n, zero, hs, m);
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.sx(), n, zero, ssb, m);
     } else {
-      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.hx(), n, zero, tmp2m.get(), m);
-      convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(tmp2m.get(), hs, (long long)m * m);
-      ++rt.prof.launches;
-      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, one, blk.x(), n, blk.sx(), n, zero, tmp2m.get(), m);
-      convert_kernel<float2, double2><<<ceil_div((long long)m * m, 256), 256, 0, rt.stream>>>(tmp2m.get(), ssb, (long long)m * m);
-      ++rt.prof.launches;
+      gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, blk.x(), n, blk.hx(), n, hs, m);
+      gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, blk.x(), n, blk.sx(), n, ssb, m);
     }
     ss.hegvd(hs, ssb, m, sc.w.get(), m);
     to_r(hs, m, blk.Y.get(), m, m, m);
@@ -383,6 +383,7 @@ struct AccRun {
     HALF_CUDA(cudaMemcpyAsync(norms.data(), sc.norms.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
     ss.status_async(infos);
     HALF_CUDA(cudaStreamSynchronize(rt.stream));
+    if constexpr (sizeof(R) == 4) tc_check(rt);
     mark("residual");
     if (infos[0] != 0) fail(kInternal, "ACC correction metric eigensolve failed (info " + std::to_string(infos[0]) + ")");
     if (infos[1] != 0) fail(kInternal, "ACC small generalized eigensolve failed (info " + std::to_string(infos[1]) + ")");
@@ -434,13 +435,8 @@ struct AccRun {
     // Rayleigh-Ritz on Z = [X PU]
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
-    if constexpr (sizeof(R) == 8) {
-      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs, hs);
-      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb, ssb);
-    } else {
-      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, tmp2m.get(), hs);
-      project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, tmp2m.get(), ssb);
-    }
+    project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs);
+    project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb);
     mark("rr_gemm");
     ss.hegvd(hs, ssb, ord, sc.w.get(), m);
     mark("hegvd");
@@ -465,10 +461,7 @@ struct AccRun {
     if constexpr (sizeof(R) == 8) {
       gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, blk.P.get(), n, blk.SP.get(), n, zero, metric, np);
     } else {
-      gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, one, blk.P.get(), n, blk.SP.get(), n, zero, blk.small.get(), np);
-      convert_kernel<float2, double2><<<ceil_div((long long)np * np, 256), 256, 0, rt.stream>>>(blk.small.get(), metric,
-                                                                                                 (long long)np * np);
-      ++rt.prof.launches;
+      gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, blk.P.get(), n, blk.SP.get(), n, metric, np);
     }
     mark("metric_gemm");
     if (!(ss.own && ss.eig.metric_normalize(rt, metric, np, ss.info.get()))) {

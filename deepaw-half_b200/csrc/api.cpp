@@ -20,6 +20,7 @@
 #include "../../include/half_b200.h"
 #include "context.h"
 #include "devmem.h"
+#include "tc_gemm.h"
 
 using namespace hb;
 
@@ -160,6 +161,9 @@ void end_call(Runtime& rt, SolveInfo& info) {
   info.sweep_ms = pf.sweep_ms;
   info.sweep_columns = pf.sweep_columns;
   info.adjoint_ms = pf.adjoint_ms;
+  info.tensor_ms = pf.tensor_ms;
+  info.tensor_flops = pf.tensor_flops;
+  info.tensor_launches = pf.tensor_launches;
 }
 
 // Solve one k point with the context's solver on runtime rt; out holds device vectors.
@@ -206,6 +210,9 @@ void accumulate(SolveInfo& total, const SolveInfo& s, bool first) {
   total.launches += s.launches;
   total.sweep_ms += s.sweep_ms;
   total.sweep_columns += s.sweep_columns;
+  total.tensor_ms += s.tensor_ms;
+  total.tensor_flops += s.tensor_flops;
+  total.tensor_launches += s.tensor_launches;
 }
 
 }  // namespace
@@ -431,7 +438,12 @@ int half_apply_hs(half_handle handle, const double kpoint[3], int nstates, int64
                                 cudaMemcpyHostToDevice, st));
     ctx->last = SolveInfo();
     begin_call(*ctx->rt);
-    apply_hs<double>(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
+    if (fp32) {
+      apply_hs_fp32(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
+      tc_check(*ctx->rt);
+    } else {
+      apply_hs<double>(*ctx, *ks, x.get(), n, nstates, hx.get(), sx.get(), ctx->acc.block);
+    }
     end_call(*ctx->rt, ctx->last);
     HALF_CUDA(cudaMemcpy2DAsync(hpsi, ld * sizeof(double2), hx.get(), n * sizeof(double2), n * sizeof(double2), nstates,
                                 cudaMemcpyDeviceToHost, st));
@@ -575,6 +587,9 @@ int half_get_last_solve_info(half_handle handle, half_solve_info_v1* info, char*
   info->sweep_ms = s.sweep_ms;
   info->sweep_columns = s.sweep_columns;
   info->adjoint_ms = s.adjoint_ms;
+  info->tensor_ms = s.tensor_ms;
+  info->tensor_flops = s.tensor_flops;
+  info->tensor_launches = s.tensor_launches;
   std::memset(info->reserved, 0, sizeof(info->reserved));
   return HALF_SUCCESS;
 }
@@ -734,8 +749,16 @@ int half_set_positions_noalloc(half_handle handle, const double* positions, char
     for (int i = 0; i < 3 * n; ++i)
       if (!std::isfinite(positions[i])) fail(kInvalidArgument, "positions must be finite");
     ctx->rebuild_dij_fixed_scratch(true);   // capacity errors leave the context unchanged
+    // The rebuild stages the new D_ij and commits it only after every species
+    // succeeded; on any error the old positions come back with it.
+    std::vector<double> old = ctx->crystal.positions;
     ctx->crystal.positions.assign(positions, positions + 3 * n);
-    ctx->rebuild_dij_fixed_scratch(false);
+    try {
+      ctx->rebuild_dij_fixed_scratch(false);
+    } catch (...) {
+      ctx->crystal.positions = std::move(old);
+      throw;
+    }
     return HALF_SUCCESS;
   });
 }
@@ -1039,4 +1062,66 @@ extern "C" int half_occupations(int nk, int nbands, const double* eigenvalues, c
     }
     return HALF_SUCCESS;
   });
+}
+
+// ---- diagnostic: the tensor-core complex GEMM on caller device memory
+namespace {
+
+std::mutex g_diag_mutex;
+
+// One runtime (stream + handles) per device for diagnostic calls; kept for
+// the life of the process.
+Runtime& diagnostic_runtime() {
+  static Runtime* rts[64] = {};
+  int dev = 0;
+  HALF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) fail(kInternal, "device ordinal out of range");
+  if (!rts[dev]) rts[dev] = new Runtime();
+  return *rts[dev];
+}
+
+bool gemm_op(char c, cublasOperation_t& op) {
+  switch (c) {
+    case 'N': case 'n': op = CUBLAS_OP_N; return true;
+    case 'T': case 't': op = CUBLAS_OP_T; return true;
+    case 'C': case 'c': op = CUBLAS_OP_C; return true;
+    default: return false;
+  }
+}
+
+}  // namespace
+
+extern "C" int half_tc_cgemm(char op_a, char op_b, int m, int n, int k, const double* alpha, const float* a,
+                             int64_t lda, const float* b, int64_t ldb, const double* beta, void* c, int64_t ldc,
+                             int c_fp64, char* error, int cap) {
+  clear_error(error, cap);
+  return guarded(error, cap, [&]() -> int {
+    cublasOperation_t ta, tb;
+    if (!gemm_op(op_a, ta) || !gemm_op(op_b, tb)) fail(kInvalidArgument, "operation must be 'N', 'T' or 'C'");
+    if (m < 0 || n < 0 || k < 0 || !alpha || !beta) fail(kInvalidArgument, "invalid GEMM dimensions or scalars");
+    if (m == 0 || n == 0) return HALF_SUCCESS;
+    const long long arows = ta == CUBLAS_OP_N ? m : k, brows = tb == CUBLAS_OP_N ? k : n;
+    if (lda < std::max(1LL, arows) || ldb < std::max(1LL, brows) || ldc < m)
+      fail(kCapacity, "leading dimension is too small");
+    if ((k > 0 && (!device_pointer(a) || !device_pointer(b))) || !device_pointer(c))
+      fail(kInvalidArgument, "operands must be device memory");
+    std::lock_guard<std::mutex> lock(g_diag_mutex);
+    Runtime& rt = diagnostic_runtime();
+    rt.prof.reset();   // the profiler's events are reused call after call
+    const float2* A = reinterpret_cast<const float2*>(a);
+    const float2* B = reinterpret_cast<const float2*>(b);
+    tc_cgemm(rt, tc_dense_a(ta, A, lda, m, k), tc_dense_b(tb, B, ldb, k, n), m, n, k, make_double2(alpha[0], alpha[1]),
+             make_double2(beta[0], beta[1]), c, c_fp64 != 0, ldc);
+    tc_check(rt);
+    return HALF_SUCCESS;
+  });
+}
+
+extern "C" int half_get_allocation_counts(int64_t* requests, int64_t* driver_allocations, char* error, int cap) {
+  clear_error(error, cap);
+  long long r = 0, d = 0;
+  device_alloc_counts(&r, &d);
+  if (requests) *requests = r;
+  if (driver_allocations) *driver_allocations = d;
+  return HALF_SUCCESS;
 }

@@ -35,6 +35,9 @@ struct SolveInfo {
   double sweep_ms = 0;           // CUDA-event time of whole H/S applications
   long long sweep_columns = 0;
   double adjoint_ms = 0;         // CUDA-event time of the force adjoint
+  double tensor_ms = 0;          // CUDA-event time of the tensor-core GEMM kernels
+  double tensor_flops = 0;       // their bf16 tensor flops (24 per complex multiply-add)
+  long long tensor_launches = 0;
 };
 
 // Event-based accounting of the library's own kernels.
@@ -42,16 +45,16 @@ struct SolveInfo {
 // synchronisation; their durations are read once, when the call ends and its
 // stream has been synchronised (collect), so timing adds no bubbles.
 struct Profile {
-  enum Kind { kLocal = 0, kSweep = 1, kAdjoint = 2 };
+  enum Kind { kLocal = 0, kSweep = 1, kAdjoint = 2, kTensor = 3 };
   cudaEvent_t a = nullptr, b = nullptr;
   std::vector<cudaEvent_t> pool;                         // reused across calls
   std::vector<std::pair<int, std::pair<int, int>>> spans;   // (kind, (begin, end) pool slots)
   size_t used = 0;
-  double local_ms = 0, local_bytes = 0, sweep_ms = 0, adjoint_ms = 0;
-  long long local_columns = 0, launches = 0, sweep_columns = 0;
+  double local_ms = 0, local_bytes = 0, sweep_ms = 0, adjoint_ms = 0, tensor_ms = 0, tensor_flops = 0;
+  long long local_columns = 0, launches = 0, sweep_columns = 0, tensor_launches = 0;
   void reset() {
-    local_ms = local_bytes = sweep_ms = adjoint_ms = 0;
-    local_columns = launches = sweep_columns = 0;
+    local_ms = local_bytes = sweep_ms = adjoint_ms = tensor_ms = tensor_flops = 0;
+    local_columns = launches = sweep_columns = tensor_launches = 0;
     spans.clear();
     used = 0;
   }
@@ -67,8 +70,9 @@ struct Runtime {
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
   bool bf16x9 = false;   // cuBLAS offers FP32 emulation on BF16 tensor cores
-  bool tc_split = true;  // large complex FP32 GEMMs as split BF16 tensor-core GEMMs (blas_split.cu)
-  DeviceBuffer<unsigned char> split_a, split_b, split_c;   // their packed operands, grow-only
+  bool tc_gemm = true;   // complex FP32 GEMMs on the library's tcgen05 kernel (tc_gemm.cu)
+  DeviceBuffer<unsigned char> tc_work;   // its split-K partial sums, grow-only
+  DeviceBuffer<int> tc_err;              // raised when one of its pipeline waits gave up
   Profile prof;
   Runtime();
   ~Runtime();
@@ -191,6 +195,10 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
 template <typename R>
 void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, int nb, cplx_t<R>* hx,
               cplx_t<R>* sx, int chunk);
+// The mixed mode's FP32 operator on complex128 device blocks (ld = n): rounded
+// to FP32, applied, widened back.  Synchronises the stream.
+void apply_hs_fp32(Context& ctx, KOperatorSet& ks, const double2* x, long long n, int nb, double2* hx, double2* sx,
+                   int chunk);
 
 // ----------------------------------------------------------------- solvers
 struct SolveOutput {

@@ -1,6 +1,8 @@
 // Caching device allocator (see devmem.h).
 #include "devmem.h"
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -58,6 +60,7 @@ struct ThreadCache {
 };
 
 thread_local ThreadCache t_cache;
+std::atomic<long long> g_requests{0}, g_driver_allocs{0};
 
 void release_all_locked() {
   for (auto& kv : g_pool) timed_free(kv.second, kv.first.second);
@@ -67,6 +70,7 @@ void release_all_locked() {
 }  // namespace
 
 void* device_alloc(size_t bytes, size_t* granted) {
+  g_requests.fetch_add(1, std::memory_order_relaxed);
   int dev = 0;
   cudaGetDevice(&dev);
   const Key key{dev, round_bytes(bytes)};
@@ -82,12 +86,14 @@ void* device_alloc(size_t bytes, size_t* granted) {
   cudaError_t e;
   {
     AllocTimer timer("cudaMalloc", key.second);
+    g_driver_allocs.fetch_add(1, std::memory_order_relaxed);
     e = cudaMalloc(&p, key.second);
   }
   if (e != cudaSuccess) {   // give the cache back and retry once
     cudaGetLastError();
     device_cache_release();
     AllocTimer timer("cudaMalloc", key.second);
+    g_driver_allocs.fetch_add(1, std::memory_order_relaxed);
     e = cudaMalloc(&p, key.second);
   }
   if (e != cudaSuccess) {
@@ -108,6 +114,11 @@ void device_free(void* p, size_t granted) {
   cudaGetDevice(&dev);
   t_cache.pool.insert({Key{dev, granted}, p});
   t_cache.bytes += granted;
+}
+
+void device_alloc_counts(long long* requests, long long* driver_allocations) {
+  if (requests) *requests = g_requests.load(std::memory_order_relaxed);
+  if (driver_allocations) *driver_allocations = g_driver_allocs.load(std::memory_order_relaxed);
 }
 
 void device_cache_release() {

@@ -22,5 +22,8 @@ namespace hb {
 void* device_alloc(size_t bytes, size_t* granted);   // throws hb::Error on failure
 void device_free(void* p, size_t granted);
 void device_cache_release();                          // return cached blocks to the driver
+// Process-wide counts since start: device_alloc calls (cached or not) and the
+// cudaMalloc calls among them.
+void device_alloc_counts(long long* requests, long long* driver_allocations);
 
 }  // namespace hb

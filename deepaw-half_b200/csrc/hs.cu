@@ -19,7 +19,12 @@
 // Bands go through in chunks (the ACC block size) so the plane buffer of a
 // chunk stays resident in the 126 MB L2 between the three kernels.  The
 // projector part is one GEMM B^H X over all species and bands, a D/Q mixing
-// kernel and two GEMMs accumulating into H X and S X.
+// kernel and the GEMMs accumulating B DY into H X and B QY into S X.  In FP64
+// B is stored and the GEMMs are cuBLAS ZGEMM (the reference's calls); in FP32
+// B is never stored: the tensor-core GEMM (tc_gemm.cu) generates its tiles
+// from a per-k radial-angular table (Omega^-1/2 beta_l(|q|) Y_lm, one row per
+// species channel), the packed plane-wave indices and the ions' b_j.R / 2 pi,
+// and B [DY | QY] is one GEMM with a doubled N writing H X and S X.
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -39,7 +44,14 @@ struct KOperator {
   DeviceBuffer<R> kinetic;
   DeviceBuffer<C> work;      // chunk x nplanes x n2 x n3
   int work_chunk = 0;
-  DeviceBuffer<C> B;         // npw x np, column-major
+  DeviceBuffer<C> B;         // FP64: npw x np, column-major
+  // FP32: the projector matrix is generated inside the tensor-core GEMM tiles
+  // (tc_gemm.cu) from these tables instead of being stored
+  DeviceBuffer<float> ftab;  // [frow][npw] Omega^-1/2 beta_l(|q|) Y_lm(q^), frow = (species, channel, m)
+  DeviceBuffer<int> gpack;   // npw packed (n1, n2, n3)
+  DeviceBuffer<int> pcol;    // np: (ion << 16) | (frow << 2) | l
+  DeviceBuffer<double> afrac;   // nions x 3: b_j . R / 2 pi
+  double kf[3] = {0, 0, 0};
   DeviceBuffer<R> dall, qall;            // D per atom, Q per species
   DeviceBuffer<int> col_base, col_a, col_nlm, col_dofs, col_qofs;
   DeviceBuffer<C> coeff, dy, qy;
@@ -237,6 +249,21 @@ struct ProjCol {
   double gmax;
 };
 
+// beta_l(|q|) Y_lm(q^) of one projector channel at one plane wave, with the
+// reference's 0.99 gmax cut (src/half_paw.F90:52-65).
+__device__ __forceinline__ double radial_angular(const ProjCol& col, double qx, double qy, double qz,
+                                                 const double* __restrict__ ry, const double* __restrict__ rm2) {
+  double qn = sqrt(qx * qx + qy * qy + qz * qz);
+  double theta = 0, phi = 0;
+  if (qn > 1.0e-10) {
+    theta = acos(fmax(-1.0, fmin(1.0, qz / qn)));
+    phi = atan2(qy, qx);
+  }
+  double rval = spline_eval(ry + col.chan * 100, rm2 + col.chan * 100, 100, col.gmax, qn);
+  if (qn > 0.99 * col.gmax) rval = 0;
+  return rval * real_ylm(col.l, col.m, cos(theta), phi);
+}
+
 // B[g, p] = Omega^-1/2 (-i)^l beta_l(|q|) Y_lm(q^) exp(-i q.R)   (src/half_paw.F90:52-65)
 __global__ void projector_kernel(double2* __restrict__ B, int npw, const double* __restrict__ q,
                                  const ProjCol* __restrict__ cols, const double* __restrict__ ry,
@@ -246,19 +273,10 @@ __global__ void projector_kernel(double2* __restrict__ B, int npw, const double*
   if (g >= npw) return;
   const ProjCol col = cols[p];
   double qx = q[3 * g], qy = q[3 * g + 1], qz = q[3 * g + 2];
-  double qn = sqrt(qx * qx + qy * qy + qz * qz);
-  double theta = 0, phi = 0;
-  if (qn > 1.0e-10) {
-    theta = acos(fmax(-1.0, fmin(1.0, qz / qn)));
-    phi = atan2(qy, qx);
-  }
-  double rval = spline_eval(ry + col.chan * 100, rm2 + col.chan * 100, 100, col.gmax, qn);
-  if (qn > 0.99 * col.gmax) rval = 0;
-  double ylm = real_ylm(col.l, col.m, cos(theta), phi);
   double ph = qx * pos[3 * col.ion] + qy * pos[3 * col.ion + 1] + qz * pos[3 * col.ion + 2];
   double s, c;
   sincos(ph, &s, &c);
-  double amp = pref * rval * ylm;
+  double amp = pref * radial_angular(col, qx, qy, qz, ry, rm2);
   // (-i)^l * (cos - i sin)
   double re = amp * c, im = -amp * s, tr, ti;
   switch (col.l & 3) {
@@ -270,9 +288,15 @@ __global__ void projector_kernel(double2* __restrict__ B, int npw, const double*
   B[(long long)p * npw + g] = make_double2(tr, ti);
 }
 
-__global__ void to_float_kernel(const double2* __restrict__ in, float2* __restrict__ out, long long n) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) out[i] = make_float2(float(in[i].x), float(in[i].y));
+// ftab[r][g] = Omega^-1/2 beta_l(|q|) Y_lm(q^) for the channel rows of the
+// generated FP32 projector tiles (one row per (species, channel, m)).
+__global__ void radial_angular_table_kernel(float* __restrict__ ftab, int npw, const double* __restrict__ q,
+                                            const ProjCol* __restrict__ rows, const double* __restrict__ ry,
+                                            const double* __restrict__ rm2, double pref) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = blockIdx.y;
+  if (g >= npw) return;
+  ftab[(long long)r * npw + g] = float(pref * radial_angular(rows[r], q[3 * g], q[3 * g + 1], q[3 * g + 2], ry, rm2));
 }
 
 template <typename R>
@@ -327,10 +351,22 @@ HostGeom plane_geometry(const Basis& b, const AxisPlan& ax, const AxisPlan& ay, 
   return h;
 }
 
+// What the FP32 operator needs to generate projector tiles: one radial-angular
+// row per (species, channel, m), the column descriptors, and the ions' b_j.R / 2 pi.
+struct ProjGen {
+  std::vector<ProjCol> frows;
+  std::vector<int> pcol;
+  std::vector<double> afrac;
+  const double* qvec = nullptr;   // device npw x 3
+  const double* ry = nullptr;     // device radial tables
+  const double* rm2 = nullptr;
+  double pref = 0;
+};
+
 template <typename R>
 void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom& hg, const DeviceBuffer<double2>& B64, int np,
                    const std::vector<int>& cb, const std::vector<int>& ca, const std::vector<int>& cn,
-                   const std::vector<int>& cd, const std::vector<int>& cq, KOperator<R>& op) {
+                   const std::vector<int>& cd, const std::vector<int>& cq, const ProjGen& gen, KOperator<R>& op) {
   cudaStream_t s = rt.stream;
   op.npw = int(basis.npw());
   op.n1 = basis.shape[0]; op.n2 = basis.shape[1]; op.n3 = basis.shape[2];
@@ -354,9 +390,22 @@ void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom
   if constexpr (sizeof(R) == 8) {
     op.B.resize(B64.size());
     HALF_CUDA(cudaMemcpyAsync(op.B.get(), B64.get(), B64.size() * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-  } else {
-    op.B.resize(B64.size());
-    to_float_kernel<<<ceil_div((long long)B64.size(), 256), 256, 0, s>>>(B64.get(), op.B.get(), (long long)B64.size());
+  } else if (np > 0) {
+    const int npw = int(basis.npw()), nf = int(gen.frows.size());
+    DeviceBuffer<ProjCol> drows;
+    drows.upload(gen.frows, s);
+    op.ftab.resize(size_t(nf) * npw);
+    radial_angular_table_kernel<<<dim3(ceil_div(npw, 256), nf), 256, 0, s>>>(op.ftab.get(), npw, gen.qvec, drows.get(),
+                                                                            gen.ry, gen.rm2, gen.pref);
+    HALF_LAUNCH("radial-angular table");
+    std::vector<int> gp(npw);
+    for (int g = 0; g < npw; ++g)
+      gp[g] = (basis.gvec[3 * g] & 1023) | ((basis.gvec[3 * g + 1] & 1023) << 10) | ((basis.gvec[3 * g + 2] & 1023) << 20);
+    op.gpack.upload(gp, s);
+    op.pcol.upload(gen.pcol, s);
+    op.afrac.upload(gen.afrac, s);
+    for (int j = 0; j < 3; ++j) op.kf[j] = basis.kpoint[j];
+    HALF_CUDA(cudaStreamSynchronize(s));   // drows is released on return
   }
   std::vector<double> dall, qall;
   for (auto& sp : ctx.species) {
@@ -427,6 +476,34 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
   }
   const int np = int(cols.size());
   ks->np = np;
+  // generated-tile tables for the FP32 operator: radial-angular rows are per
+  // (species, channel, m), shared by the species' atoms
+  ProjGen gen;
+  {
+    int chan = 0, frow0 = 0;
+    size_t c = 0;
+    for (auto& sp : ctx.species) {
+      for (int ch = 0; ch < sp.nchan; ++ch) {
+        int l = sp.lps[ch];
+        for (int m = -l; m <= l; ++m) gen.frows.push_back({chan + ch, l, m, 0, sp.pspnl_gmax});
+      }
+      for (int a = 0; a < sp.natoms; ++a)
+        for (int ilm = 0; ilm < sp.nlm; ++ilm, ++c) {
+          if (cols[c].ion >= (1 << 15) || frow0 + ilm >= (1 << 14)) fail(kUnavailable, "too many ions or projector channels");
+          gen.pcol.push_back((cols[c].ion << 16) | ((frow0 + ilm) << 2) | (cols[c].l & 3));
+        }
+      chan += sp.nchan;
+      frow0 += sp.nlm;
+    }
+    auto rec = ctx.crystal.reciprocal();
+    for (int i = 0; i < ctx.crystal.nions(); ++i) {
+      auto r = ctx.crystal.cartesian(i);
+      for (int j = 0; j < 3; ++j)
+        gen.afrac.push_back((rec[3 * j] * r[0] + rec[3 * j + 1] * r[1] + rec[3 * j + 2] * r[2]) / (2.0 * kPi));
+    }
+  }
+  for (size_t g = 0; g < basis.gvec.size(); ++g)
+    if (basis.gvec[g] < -512 || basis.gvec[g] > 511) fail(kUnavailable, "plane-wave index beyond the packed range");
   ks->qvec.upload(basis.qvec, s);
   DeviceBuffer<ProjCol> dcols;
   dcols.upload(cols, s);
@@ -435,6 +512,10 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
   drm2.upload(rm2, s);
   dpos.upload(pos, s);
   DeviceBuffer<double2> B64((size_t)npw * np);
+  gen.qvec = ks->qvec.get();
+  gen.ry = dry.get();
+  gen.rm2 = drm2.get();
+  gen.pref = 1.0 / std::sqrt(ctx.crystal.volume());
   if (np > 0) {
     projector_kernel<<<dim3(ceil_div(npw, 256), np), 256, 0, s>>>(B64.get(), npw, ks->qvec.get(), dcols.get(), dry.get(),
                                                                    drm2.get(), dpos.get(), 1.0 / std::sqrt(ctx.crystal.volume()));
@@ -442,11 +523,11 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
   }
   if (fp64) {
     ks->op64 = std::make_unique<KOperator<double>>();
-    fill_operator<double>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op64);
+    fill_operator<double>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, gen, *ks->op64);
   }
   if (fp32) {
     ks->op32 = std::make_unique<KOperator<float>>();
-    fill_operator<float>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, *ks->op32);
+    fill_operator<float>(ctx, rt, basis, hg, B64, np, cb, ca, cn, cd, cq, gen, *ks->op32);
   }
   HALF_CUDA(cudaStreamSynchronize(s));
   return ks;
@@ -529,18 +610,78 @@ void apply_nonlocal(Runtime& rt, KOperator<R>& op, const cplx_t<R>* x, long long
     op.ws_cols = nb;
   }
   const C one = cval<R>(1.0), zero = cval<R>(0.0);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, op.np, nb, op.npw, one, op.B.get(), op.npw, x, ld, zero, op.coeff.get(), op.np);
-  mix_kernel<R><<<ceil_div((long long)op.np * nb, 256), 256, 0, s>>>(op.coeff.get(), op.np, nb, op.col_base.get(),
-                                                                     op.col_a.get(), op.col_nlm.get(), op.col_dofs.get(),
-                                                                     op.col_qofs.get(), op.dall.get(), op.qall.get(),
-                                                                     op.dy.get(), op.qy.get());
-  HALF_LAUNCH("mix");
-  gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.dy.get(), op.np, one, hx, ld);
-  gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.qy.get(), op.np, one, sx, ld);
+  auto mix = [&]() {
+    mix_kernel<R><<<ceil_div((long long)op.np * nb, 256), 256, 0, s>>>(op.coeff.get(), op.np, nb, op.col_base.get(),
+                                                                       op.col_a.get(), op.col_nlm.get(), op.col_dofs.get(),
+                                                                       op.col_qofs.get(), op.dall.get(), op.qall.get(),
+                                                                       op.dy.get(), op.qy.get());
+    HALF_LAUNCH("mix");
+    ++rt.prof.launches;
+  };
+  if constexpr (sizeof(R) == 4) {
+    // FP32: B is generated inside the tensor-core tiles (tc_gemm.cu).
+    //   coeff = conj(B)^T X            (np x nb, K = npw)
+    //   [H X | S X] += B [DY | QY]     (npw x 2nb, K = np; one GEMM, two outputs)
+    TcOperand bh;
+    bh.kind = TcOperand::kProjConj;
+    bh.rows = op.np;
+    bh.kdim = op.npw;
+    bh.ftab = op.ftab.get();
+    bh.gpack = op.gpack.get();
+    bh.pcol = op.pcol.get();
+    bh.afrac = op.afrac.get();
+    bh.kf0 = op.kf[0];
+    bh.kf1 = op.kf[1];
+    bh.kf2 = op.kf[2];
+    bh.npw = op.npw;
+    tc_cgemm(rt, bh, tc_dense_b(CUBLAS_OP_N, x, ld, op.npw, nb), op.np, nb, op.npw, make_double2(1, 0),
+             make_double2(0, 0), op.coeff.get(), false, op.np);
+    mix();
+    TcOperand b = bh;
+    b.kind = TcOperand::kProj;
+    b.rows = op.npw;
+    b.kdim = op.np;
+    TcOperand y = tc_dense_b(CUBLAS_OP_N, op.dy.get(), op.np, op.np, 2 * nb);
+    y.p2 = op.qy.get();
+    y.split = nb;
+    tc_cgemm(rt, b, y, op.npw, 2 * nb, op.np, make_double2(1, 0), make_double2(1, 0), hx, false, ld, sx, nb);
+  } else {
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, op.np, nb, op.npw, one, op.B.get(), op.npw, x, ld, zero, op.coeff.get(), op.np);
+    mix();
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.dy.get(), op.np, one, hx, ld);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, op.npw, nb, op.np, one, op.B.get(), op.npw, op.qy.get(), op.np, one, sx, ld);
+  }
 }
 
 template void apply_hs<double>(Context&, KOperatorSet&, const double2*, long long, int, double2*, double2*, int);
 template void apply_hs<float>(Context&, KOperatorSet&, const float2*, long long, int, float2*, float2*, int);
+
+namespace {
+template <typename A, typename B>
+__global__ void convert_complex_kernel(const A* __restrict__ in, B* __restrict__ out, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) {
+    B v;
+    v.x = in[i].x;
+    v.y = in[i].y;
+    out[i] = v;
+  }
+}
+}  // namespace
+
+void apply_hs_fp32(Context& ctx, KOperatorSet& ks, const double2* x, long long n, int nb, double2* hx, double2* sx,
+                   int chunk) {
+  cudaStream_t s = ks.rt->stream;
+  const long long tot = n * nb;
+  DeviceBuffer<float2> x32(tot), h32(tot), s32(tot);
+  convert_complex_kernel<double2, float2><<<ceil_div(tot, 256), 256, 0, s>>>(x, x32.get(), tot);
+  HALF_LAUNCH("to FP32");
+  apply_hs<float>(ctx, ks, x32.get(), n, nb, h32.get(), s32.get(), chunk);
+  convert_complex_kernel<float2, double2><<<ceil_div(tot, 256), 256, 0, s>>>(h32.get(), hx, tot);
+  convert_complex_kernel<float2, double2><<<ceil_div(tot, 256), 256, 0, s>>>(s32.get(), sx, tot);
+  HALF_LAUNCH("to FP64");
+  HALF_CUDA(cudaStreamSynchronize(s));
+}
 
 void accumulate_band_density(KOperatorSet& ks, const double2* x, long long ld, int nb, const double* bw,
                              double* density_c, int chunk) {

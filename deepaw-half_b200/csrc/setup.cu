@@ -39,7 +39,7 @@ Runtime::Runtime() {
   if (bf16x9 && cublasSetMathMode(blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) != CUBLAS_STATUS_SUCCESS) bf16x9 = false;
   HALF_CUDA(cudaEventCreate(&prof.a));
   HALF_CUDA(cudaEventCreate(&prof.b));
-  if (const char* sp = std::getenv("HALF_TC_SPLIT")) tc_split = std::string(sp) != "0";
+  if (const char* tg = std::getenv("HALF_TC_GEMM")) tc_gemm = std::string(tg) != "0";
 }
 
 int Profile::record(cudaStream_t s) {
@@ -58,6 +58,7 @@ void Profile::collect() {
     HALF_CUDA(cudaEventElapsedTime(&ms, pool[sp.second.first], pool[sp.second.second]));
     if (sp.first == kLocal) local_ms += ms;
     else if (sp.first == kSweep) sweep_ms += ms;
+    else if (sp.first == kTensor) tensor_ms += ms;
     else adjoint_ms += ms;
   }
   spans.clear();
@@ -709,6 +710,9 @@ std::mutex g_fixed_mutex;
 unsigned char* g_fixed_addr[kMaxDevices] = {};
 
 // Address of the scratch on the current device, resolved once per device.
+// The cached address belongs to the device's primary context, which the
+// library assumes lives as long as the process: after a cudaDeviceReset the
+// next call would use a stale address.
 unsigned char* fixed_scratch() {
   int dev = 0;
   HALF_CUDA(cudaGetDevice(&dev));
@@ -758,10 +762,13 @@ int fixed_chunk(const SpeciesDevice& sp, size_t region) {
 void Context::rebuild_dij_fixed_scratch(bool check_only) {
   cudaStream_t s = rt->stream;
   if (!use_uspp) {   // DION only: copies into the existing D buffers
+    for (auto& sp : species) {
+      const size_t nd = size_t(sp.natoms) * sp.tables.dion_lm.size();
+      if (sp.dij.size() != nd || sp.ddij.size() != 3 * nd) fail(kInternal, "D_ij buffers were not set up");
+    }
     if (check_only) return;
     for (auto& sp : species) {
       const size_t per = sp.tables.dion_lm.size(), nd = size_t(sp.natoms) * per;
-      if (sp.dij.size() != nd || sp.ddij.size() != 3 * nd) fail(kInternal, "D_ij buffers were not set up");
       sp.dij_host.resize(nd);
       for (int a = 0; a < sp.natoms; ++a)
         std::copy(sp.tables.dion_lm.begin(), sp.tables.dion_lm.end(), sp.dij_host.begin() + a * per);
@@ -772,13 +779,17 @@ void Context::rebuild_dij_fixed_scratch(bool check_only) {
     return;
   }
   const long long n = nr();
+  // The new D_ij and dD_ij/dR of every species are staged at the end of the
+  // scratch and copied into the context only after every species succeeded.
+  size_t stage_bytes = 0;
+  for (auto& sp : species) stage_bytes += align256(size_t(sp.natoms) * sp.nlm * sp.nlm * 4 * sizeof(double));
   const size_t coeff_bytes = align256(size_t(n) * sizeof(double));
-  const size_t need_fft = coeff_bytes + align256(size_t(n) * sizeof(double2));
+  const size_t need_fft = coeff_bytes + align256(size_t(n) * sizeof(double2)) + stage_bytes;
   if (need_fft > kFixedScratchBytes)
     fail(kCapacity, "the fixed D_ij scratch holds " + std::to_string(kFixedScratchBytes >> 20) + " MiB; a " +
                         std::to_string(n) + "-point grid needs " + std::to_string(need_fft) +
-                        " bytes (24 B per point): use half_set_positions");
-  const size_t region = kFixedScratchBytes - coeff_bytes;
+                        " bytes (24 B per point plus the staged D_ij): use half_set_positions");
+  const size_t region = kFixedScratchBytes - coeff_bytes - stage_bytes;
   std::vector<int> chunk(species.size());
   for (size_t it = 0; it < species.size(); ++it) {
     chunk[it] = fixed_chunk(species[it], region);
@@ -794,6 +805,15 @@ void Context::rebuild_dij_fixed_scratch(bool check_only) {
 
   unsigned char* base = fixed_scratch();
   double* coeff = reinterpret_cast<double*>(base);
+  unsigned char* stage = base + kFixedScratchBytes - stage_bytes;
+  std::vector<double*> stage_d(species.size());
+  {
+    size_t off = 0;
+    for (size_t it = 0; it < species.size(); ++it) {
+      stage_d[it] = reinterpret_cast<double*>(stage + off);
+      off += align256(size_t(species[it].natoms) * species[it].nlm * species[it].nlm * 4 * sizeof(double));
+    }
+  }
   double2* freq = reinterpret_cast<double2*>(base + coeff_bytes);
   const auto& sh = charge.shape;
   real_to_complex_kernel<<<blocks_for(n), 256, 0, s>>>(veff.get(), freq, n, 1.0);
@@ -849,12 +869,21 @@ void Context::rebuild_dij_fixed_scratch(bool check_only) {
                                                                      ncomp, radial);
       HALF_LAUNCH("qdep radial");
       const long long npair = (long long)na * nd;
+      double* sd = stage_d[it];
+      double* sdd = sd + size_t(sp.natoms) * nd;
       finish_dij_kernel<<<blocks_for(npair), 256, 0, s>>>(ddion, dmp, radial, na, sp.nlm, t.naug, ncomp,
-                                                           sp.dij.get() + a0 * nd, sp.ddij.get() + 3 * a0 * nd);
+                                                           sd + a0 * nd, sdd + 3 * a0 * nd);
       HALF_LAUNCH("qdep finish");
     }
-    HALF_CUDA(cudaMemcpyAsync(sp.dij_host.data(), sp.dij.get(), sp.dij.size() * sizeof(double),
-                              cudaMemcpyDeviceToHost, s));
+  }
+  // every species succeeded: commit the staged D_ij and dD_ij/dR
+  HALF_CUDA(cudaStreamSynchronize(s));
+  for (size_t it = 0; it < species.size(); ++it) {
+    SpeciesDevice& sp = species[it];
+    const size_t nd = size_t(sp.natoms) * sp.nlm * sp.nlm;
+    HALF_CUDA(cudaMemcpyAsync(sp.dij.get(), stage_d[it], nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    HALF_CUDA(cudaMemcpyAsync(sp.ddij.get(), stage_d[it] + nd, 3 * nd * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    HALF_CUDA(cudaMemcpyAsync(sp.dij_host.data(), stage_d[it], nd * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   HALF_CUDA(cudaStreamSynchronize(s));
 }

@@ -46,7 +46,8 @@ class SolveInfo(C.Structure):
                 ("operator_ms", C.c_double), ("device_ms", C.c_double), ("local_ms", C.c_double),
                 ("local_bytes", C.c_double), ("local_columns", C.c_int64), ("kernel_launches", C.c_int64),
                 ("sweep_ms", C.c_double), ("sweep_columns", C.c_int64), ("adjoint_ms", C.c_double),
-                ("reserved", C.c_uint64 * 4)]
+                ("tensor_ms", C.c_double), ("tensor_flops", C.c_double), ("tensor_launches", C.c_int64),
+                ("reserved", C.c_uint64 * 1)]
 
 
 class RequestGeometry(C.Structure):
@@ -97,6 +98,9 @@ _SIGS = {
     "half_occupations": (C.c_int, [C.c_int, C.c_int, _P, _P, C.c_double, C.c_double, C.c_int, _P, _P] + _ERR),
     "half_forces": (C.c_int, [C.c_int64, C.c_int, _P, _P, C.c_int, C.c_double, C.c_double, C.c_int, _P, _P, _P, _P]
                     + _ERR),
+    "half_get_allocation_counts": (C.c_int, [_P, _P] + _ERR),
+    "half_tc_cgemm": (C.c_int, [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, _P, C.c_void_p, C.c_int64, C.c_void_p,
+                                C.c_int64, _P, C.c_void_p, C.c_int64, C.c_int] + _ERR),
 }
 
 
@@ -152,6 +156,28 @@ def occupations(eigenvalues, weights, nelect, sigma, ismear=-1):
     _check(load_library().half_occupations(eig.shape[0], eig.shape[1], _ptr(eig), _ptr(w), float(nelect),
                                            float(sigma), int(ismear), _ptr(occ), _ptr(en), err, 512), err)
     return occ, en[0], en[1], en[2]
+
+
+def allocation_counts():
+    """(device buffers taken, cudaMalloc calls) since the library was loaded."""
+    lib = load_library()
+    err = C.create_string_buffer(128)
+    r, d = C.c_int64(0), C.c_int64(0)
+    _check(lib.half_get_allocation_counts(C.byref(r), C.byref(d), err, 128), err)
+    return int(r.value), int(d.value)
+
+
+def tc_cgemm(op_a, op_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc, c_fp64=False):
+    """C = alpha op(A) op(B) + beta C on the library's tensor-core kernel.
+    a_ptr, b_ptr, c_ptr: device addresses of column-major complex64 data
+    (complex128 for C when c_fp64); op_a / op_b in 'N', 'T', 'C'."""
+    lib = load_library()
+    err = C.create_string_buffer(512)
+    al = np.array([alpha.real, alpha.imag], dtype=np.float64)
+    be = np.array([beta.real, beta.imag], dtype=np.float64)
+    st = lib.half_tc_cgemm(op_a.encode(), op_b.encode(), m, n, k, _ptr(al), C.c_void_p(a_ptr), lda,
+                           C.c_void_p(b_ptr), ldb, _ptr(be), C.c_void_p(c_ptr), ldc, int(bool(c_fp64)), err, 512)
+    _check(st, err)
 
 
 class Context:

@@ -177,7 +177,9 @@ int half_get_basis(half_handle handle, const double kpoint[3], int64_t capacity,
 
 /* reference half.h:168-174.  The reference's CUDA contexts answer UNAVAILABLE
  * here; this build evaluates both on the GPU (dense assembly for
- * half_assemble_hs, the matrix-free operator for half_apply_hs). */
+ * half_assemble_hs, the matrix-free operator for half_apply_hs: FP64, or the
+ * mixed mode's FP32 operator when half_set_acc_controls selected
+ * HALF_PRECISION_MIXED). */
 int half_assemble_hs(half_handle handle, const double kpoint[3], int64_t ld,
                      HALF_C128 *h, HALF_C128 *s,
                      char *error, int error_capacity);

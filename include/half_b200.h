@@ -64,7 +64,11 @@ typedef struct half_solve_info_v1 {
   double sweep_ms;             /* CUDA-event time of whole H/S applications */
   int64_t sweep_columns;       /* band columns of those applications */
   double adjoint_ms;           /* CUDA-event time of the force adjoint (GEMM + epilogue) */
-  uint64_t reserved[4];
+  double tensor_ms;            /* CUDA-event time of the tensor-core GEMM kernels */
+  double tensor_flops;         /* their bf16 tensor flops: 24 per complex multiply-add
+                                  (four real products, three split terms) */
+  int64_t tensor_launches;     /* tensor-core GEMM kernel launches */
+  uint64_t reserved[1];
 } half_solve_info_v1;
 int half_get_last_solve_info(half_handle handle, half_solve_info_v1 *info,
                              char *error, int error_capacity);
@@ -107,13 +111,17 @@ int half_set_positions(half_handle handle, const double *positions_fractional,
  * synchronisation of cudaMalloc/cudaFree.  Results are identical to
  * half_set_positions.
  * Scratch: one fixed 32 MiB device array inside the library, shared by every
- * handle on a device.  It must hold 24 bytes per grid point plus one atom's
- * QDEP samples (about 1.5 MB); larger systems get HALF_ERROR_CAPACITY and
- * the context is left unchanged.  Nothing in it needs to start at zero.
- * Calls that overlap on one device (any handles, any threads) race on the
- * scratch: serialise them.  The first call on each device resolves the
- * scratch address (cudaGetSymbolAddress) and must not be made while a stream
- * capture is in progress. */
+ * handle on a device.  It must hold 24 bytes per grid point, the new D_ij and
+ * dD_ij/dR (32 bytes per atom and projector pair) and one atom's QDEP samples
+ * (about 1.5 MB); larger systems get HALF_ERROR_CAPACITY.  The new D_ij is
+ * staged in the scratch and copied into the context only when every species
+ * succeeded, so on any error the context keeps its positions and D_ij.
+ * Nothing in the scratch needs to start at zero.  Calls that overlap on one
+ * device (any handles, any threads) race on the scratch: serialise them.  The
+ * first call on each device resolves the scratch address
+ * (cudaGetSymbolAddress) and must not be made while a stream capture is in
+ * progress; the address is kept for the life of the process, which assumes the
+ * device's primary context is not reset (cudaDeviceReset) meanwhile. */
 int half_set_positions_noalloc(half_handle handle,
                                const double *positions_fractional,
                                char *error, int error_capacity);
@@ -229,6 +237,30 @@ int half_occupations(int nk, int nbands, const double *eigenvalues,
                      const double *kweights, double nelect, double sigma,
                      int ismear, double *occupations, double *energies,
                      char *error, int error_capacity);
+
+/* Device-memory requests of this process since it loaded the library (a
+ * diagnostic with no counterpart in the reference): *requests counts every
+ * device buffer the library took, from its cache or from the driver, and
+ * *driver_allocations the cudaMalloc calls among them.  Either pointer may be
+ * NULL.  Comparing the counts around a call shows whether it allocated. */
+int half_get_allocation_counts(int64_t *requests, int64_t *driver_allocations,
+                               char *error, int error_capacity);
+
+/* Complex FP32 GEMM on the library's tcgen05 tensor-core kernel, the kernel
+ * behind the mixed mode's projector and subspace products (a diagnostic
+ * entry; the reference's products are cuBLAS ZGEMM calls,
+ * src/half_cuda_assembly.cuf:502-512, src/half_cuda_iterative_solver.cuf:
+ * 148-194).  C = alpha op(A) op(B) + beta C with op(A) m x k, op(B) k x n;
+ * op_a / op_b are 'N', 'T' or 'C'.  a, b: device memory, column-major
+ * complex64 (interleaved float pairs); c: device memory, complex64, or
+ * complex128 when c_fp64 != 0.  Every operand is split into bf16 hi/lo
+ * parts and each real product taken as hi*hi + hi*lo + lo*hi with FP32
+ * accumulation (relative error about 2^-16).  Returns when C is complete;
+ * host pointers give HALF_ERROR_INVALID_ARGUMENT. */
+int half_tc_cgemm(char op_a, char op_b, int m, int n, int k,
+                  const double alpha[2], const float *a, int64_t lda,
+                  const float *b, int64_t ldb, const double beta[2], void *c,
+                  int64_t ldc, int c_fp64, char *error, int error_capacity);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,33 @@ def test_apply_hs_fp64(name, k, si2, hfo2, oracle_system):
     assert np.abs(sg - sr).max() <= 1e-11 * np.abs(sr).max()
 
 
+@pytest.mark.parametrize("name", ["si2", "hfo2"])
+@pytest.mark.parametrize("k", [(0, 0, 0), (0.125, -0.25, 0.375)])
+def test_apply_hs_fp32(name, k, si2, hfo2, oracle_system):
+    """The mixed mode's operator: FP32 local part, projector part on the
+    tensor cores with B generated in-tile (split bf16, 2^-16).  H psi and S psi
+    agree with the FP64 oracle to 1e-4 of their largest element, and the
+    projector part alone (S psi - psi = B Q B^H psi) to 1e-4 of its own."""
+    from oracle import hamiltonian as H
+    files = {"si2": si2, "hfo2": hfo2}[name]
+    sysm = oracle_system(name, files)
+    op = H.prepare(sysm, k)
+    r = rng(2)
+    psi = r.normal(size=(op.basis.npw, 37)) + 1j * r.normal(size=(op.basis.npw, 37))
+    hr, sr = H.apply_hs(op, psi)
+    with ctx_for(files) as ctx:
+        ctx.set_acc(precision="mixed")
+        hg, sg = ctx.apply_hs(k, psi)
+    psi32 = psi.astype(np.complex64).astype(np.complex128)
+    assert np.abs(hg - hr).max() <= 1e-4 * np.abs(hr).max()
+    assert np.abs(sg - sr).max() <= 1e-4 * np.abs(sr).max()
+    proj_ref = sr - psi
+    proj_gpu = sg - psi32
+    assert np.abs(proj_gpu - proj_ref).max() <= 1e-4 * np.abs(proj_ref).max()
+    # and it is the FP32 path, not the FP64 one
+    assert np.abs(hg - hr).max() > 1e-9 * np.abs(hr).max()
+
+
 def test_assemble_hs(si2, oracle_system):
     from oracle import hamiltonian as H
     op = H.prepare(oracle_system("si2", si2))
@@ -203,3 +230,29 @@ def test_guarded_and_mixed_match_dense_on_the_64_atom_cell(inputs_dir):
             e = ctx.solve(k, w.nbands)[0]
             assert ctx.info()["converged"] == 1
             assert np.abs(e - ref).max() <= tol, (precision, np.abs(e - ref).max())
+
+
+@pytest.mark.parametrize("name", ["si2", "hfo2"])
+def test_soft_locking_matches_dense(name, si2, hfo2, oracle_system, monkeypatch):
+    """Soft locking (HALF_SOFT_LOCK=1, guard-band modes): requested bands whose
+    residual is at or below half the tolerance add no correction direction, so
+    the Rayleigh-Ritz pencils shrink; the converged eigenvalues must still be
+    the dense solve's, and the operator must see fewer columns than without."""
+    from oracle import hamiltonian as H
+    files = {"si2": si2, "hfo2": hfo2}[name]
+    w = files[0]
+    op = H.prepare(oracle_system(name, files))
+    nb = 8 if name == "si2" else w.nbands
+    ref, _, _, _ = H.solve_dense(op, nb)
+    with ctx_for(files) as ctx:
+        for precision, tol in (("fp64_guarded", 1e-10), ("mixed", 1e-8)):
+            cols = {}
+            for lock in ("0", "1"):
+                monkeypatch.setenv("HALF_SOFT_LOCK", lock)
+                ctx.set_acc(tol=2e-5 if name == "hfo2" else 1e-7, max_iterations=400, precision=precision)
+                e, _, _, _ = ctx.solve((0, 0, 0), nb)
+                info = ctx.info()
+                assert info["converged"] == 1, (precision, lock)
+                assert np.abs(e - ref).max() <= tol, (precision, lock, np.abs(e - ref).max())
+                cols[lock] = info["operator_applications"] / max(1, info["iterations"])
+            assert cols["1"] < cols["0"], (precision, cols)

@@ -51,8 +51,13 @@ def test_noalloc_matches_set_positions_over_two_calls(name, inputs_dir):
             pos = displaced(w, seed)
             ctx.set_positions(pos)
             ref = observe(ctx, psi)
+            r0, _ = halfb200.allocation_counts()
             ctx.set_positions(w.positions)          # the next call must redo the work
+            r1, d1 = halfb200.allocation_counts()
+            assert r1 > r0                          # the allocating path takes device buffers
             ctx.set_positions_noalloc(pos)
+            r2, d2 = halfb200.allocation_counts()
+            assert (r2 - r1, d2 - d1) == (0, 0)     # this one takes none, cached or new
             got = observe(ctx, psi)
             for a, b in zip(got, ref):
                 assert np.array_equal(a, b), np.abs(a - b).max()
@@ -78,7 +83,9 @@ def test_noalloc_runs_with_less_free_memory_than_the_allocating_path_needs(input
         free, _ = torch.cuda.mem_get_info()
         hog = torch.empty(max(0, free - headroom), dtype=torch.uint8, device="cuda")
         try:
+            r0, d0 = halfb200.allocation_counts()
             ctx.set_positions_noalloc(pos)
+            assert halfb200.allocation_counts() == (r0, d0)
         finally:
             del hog
             torch.cuda.empty_cache()
