@@ -56,7 +56,7 @@ def parse():
     p.add_argument("--tol", type=float, default=2e-5,
                    help="ACC residual tolerance (eV); keeps |d eps| below 1e-8 eV against the dense solve")
     p.add_argument("--max-iter", type=int, default=2000)
-    p.add_argument("--block", type=int, default=16)
+    p.add_argument("--block", type=int, default=0, help="bands per operator chunk; 0 = the autotuner's choice")
     p.add_argument("--guarded-kpoints", type=int, default=2,
                    help="k points solved in the FP64-with-guard-bands comparison")
     p.add_argument("--fp64-max-iter", type=int, default=300,

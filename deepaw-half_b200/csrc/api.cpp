@@ -548,7 +548,7 @@ int half_set_acc_controls(half_handle handle, double tol, int max_iterations, in
   clear_error(error, cap);
   Context* ctx = lookup(handle);
   if (!ctx) return bad_handle(error, cap);
-  if (!(tol > 0) || !std::isfinite(tol) || max_iterations < 1 || block_size < 1 ||
+  if (!(tol > 0) || !std::isfinite(tol) || max_iterations < 1 || block_size < 0 ||
       (precision != HALF_PRECISION_FP64 && precision != HALF_PRECISION_MIXED &&
        precision != HALF_PRECISION_FP64_GUARDED)) {
     export_error("invalid ACC solver controls", error, cap);

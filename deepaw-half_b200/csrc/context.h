@@ -15,11 +15,14 @@ namespace hb {
 
 enum Precision : int { kFP64 = 0, kMixed = 1, kFP64Guarded = 2 };
 
-// ACC controls; the defaults are the reference's (src/half_cuda_iterative_solver.cuf:113-118).
+// ACC controls; tolerance and iteration bound default to the reference's
+// (src/half_cuda_iterative_solver.cuf:113-118).  block is the operator's bands
+// per chunk (the reference's 16); 0, the default here, lets the autotuner
+// choose it (tune.h), which changes no result.
 struct AccControls {
   double tol = 1.0e-4;
   int max_iter = 40;
-  int block = 16;
+  int block = 0;
   int precision = kFP64;
 };
 

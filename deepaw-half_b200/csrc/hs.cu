@@ -31,6 +31,7 @@
 
 #include "blas.h"
 #include "context.h"
+#include "tune.h"
 
 namespace hb {
 
@@ -558,6 +559,18 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
   Runtime& rt = *ks.rt;
   cudaStream_t s = rt.stream;
   if (nb <= 0) return;
+  // chunk <= 0: bands per chunk chosen by the autotuner (tune.h) per box,
+  // sphere extent and precision; every choice gives bit-identical results
+  int tune_token = 0;
+  if (chunk <= 0) {
+    static const std::vector<int> cand = {16, 8, 32, 64};
+    const std::string key = "local " + std::to_string(op.n1) + "x" + std::to_string(op.n2) + "x" +
+                            std::to_string(op.n3) + " planes " + std::to_string(op.nplanes) + " fp" +
+                            std::to_string(8 * sizeof(R));
+    const int idx = Tuner::pick(key, cand);
+    chunk = cand[idx];
+    tune_token = Tuner::begin(key, idx, s);
+  }
   chunk = std::max(1, std::min(chunk, nb));
   if (op.work_chunk < chunk) {
     op.work.resize((size_t)chunk * op.nplanes * op.n2 * op.n3);
@@ -581,6 +594,7 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
     pf.launches += 3;
   }
   HALF_LAUNCH("local operator");
+  Tuner::finish(tune_token, s, double(nb));
   pf.span(Profile::kLocal, ev_local, pf.record(s));
   {
     // FFT-path algorithmic bytes per band: read psi, write H psi and S psi, two
@@ -688,6 +702,7 @@ void accumulate_band_density(KOperatorSet& ks, const double2* x, long long ld, i
   KOperator<double>& op = pick<double>(ks);
   cudaStream_t s = ks.rt->stream;
   if (nb <= 0) return;
+  if (chunk <= 0) chunk = 16;
   chunk = std::max(1, std::min(chunk, nb));
   if (op.work_chunk < chunk) {
     op.work.resize((size_t)chunk * op.nplanes * op.n2 * op.n3);

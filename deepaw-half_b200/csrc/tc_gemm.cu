@@ -30,9 +30,12 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <string>
+#include <vector>
 
 #include "tc.cuh"
 #include "tc_gemm.h"
+#include "tune.h"
 
 namespace hb {
 
@@ -467,13 +470,15 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     rt.tc_err.zero(st);
   }
   if (C2 == nullptr) split_col = INT_MAX;
-  const int bn = pick_bn(N);
-  const int mt = (M + kBM - 1) / kBM, nt = (N + bn - 1) / bn;
+  // The split-K boundaries follow from the default tile width only, so the
+  // tile width the autotuner picks (tune.h) changes no result.
+  const int bn0 = pick_bn(N);
+  const int mt = (M + kBM - 1) / kBM, nt0 = (N + bn0 - 1) / bn0;
   const int nkb = (K + kBK - 1) / kBK;
   int dev = 0, sms = 148;
   HALF_CUDA(cudaGetDevice(&dev));
   HALF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const long long tiles = (long long)mt * nt;
+  const long long tiles = (long long)mt * nt0;
   int splits = 1;
   if (tiles < sms && nkb > 0) {
     splits = int(std::min<long long>((sms + tiles - 1) / tiles, std::max(1, nkb / 4)));
@@ -481,6 +486,21 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
   }
   const int kbps = nkb > 0 ? (nkb + splits - 1) / splits : 0;
   if (nkb > 0) splits = (nkb + kbps - 1) / kbps;
+  // tile width: 0, 1 or 2 more N tiles than the fewest are the candidates
+  std::vector<int> cand;
+  for (int extra = 0; extra < 3; ++extra) {
+    const int t = nt0 + extra, w = ((N + t - 1) / t + 15) / 16 * 16;
+    if (w >= 16 && (cand.empty() || w < cand.back())) cand.push_back(w);
+  }
+  int tune_token = 0, bn = bn0;
+  if (nkb > 0 && cand.size() > 1) {
+    const std::string key = "gemm " + std::to_string(A.kind) + std::to_string(B.kind) + " " + std::to_string(M) +
+                            "x" + std::to_string(N) + "x" + std::to_string(K) + " s" + std::to_string(splits);
+    const int idx = Tuner::pick(key, cand);
+    bn = cand[idx];
+    tune_token = Tuner::begin(key, idx, st);
+  }
+  const int nt = (N + bn - 1) / bn;
   const size_t smem = size_t(kStages) * stage_bytes(bn, A.kind, B.kind) + kSmemSlack;
   raise_smem_limit(tc_cgemm_kernel, smem);
   Out o{};
@@ -506,6 +526,7 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     const int e0 = pf.record(st);
     tc_cgemm_kernel<<<dim3(mt, nt, splits), kThreads, smem, st>>>(A, B, bn, kbps, nkb, o, rt.tc_err.get());
     HALF_LAUNCH("tensor-core cgemm");
+    Tuner::finish(tune_token, st, 1.0);
     pf.span(Profile::kTensor, e0, pf.record(st));
     pf.tensor_flops += 24.0 * double(M) * double(N) * double(K);
     ++pf.tensor_launches;

@@ -296,7 +296,8 @@ class Context:
         return h.T, s.T
 
     # -------------------------------------------------------------- extensions
-    def set_acc(self, tol=1e-4, max_iterations=40, block_size=16, precision="fp64"):
+    def set_acc(self, tol=1e-4, max_iterations=40, block_size=0, precision="fp64"):
+        """ACC controls; block_size 0 lets the library's autotuner pick the bands per chunk."""
         err = self._err()
         _check(self.lib.half_set_acc_controls(self.handle, float(tol), int(max_iterations), int(block_size),
                                               PRECISION[precision], err, 512), err)

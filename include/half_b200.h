@@ -34,8 +34,10 @@ enum half_precision {
  * 113-119; CLI --acc-tol, --acc-max-iter, --acc-block-size) but ABI v1 never
  * passes them, so the defaults 1e-4 eV / 40 / 16 apply (src/half_library.F90:
  * 343-367).  This setter keeps those defaults until it is called.
- * tolerance_eV > 0, max_iterations >= 1, block_size >= 1, precision one of
- * half_precision; otherwise HALF_ERROR_INVALID_ARGUMENT. */
+ * tolerance_eV > 0, max_iterations >= 1, block_size >= 0, precision one of
+ * half_precision; otherwise HALF_ERROR_INVALID_ARGUMENT.  block_size is the
+ * operator's bands per chunk; 0 (this library's default) lets its
+ * autotuner choose it by measurement, which changes no result. */
 int half_set_acc_controls(half_handle handle, double tolerance_eV,
                           int max_iterations, int block_size, int precision,
                           char *error, int error_capacity);

@@ -256,3 +256,27 @@ def test_soft_locking_matches_dense(name, si2, hfo2, oracle_system, monkeypatch)
                 assert np.abs(e - ref).max() <= tol, (precision, lock, np.abs(e - ref).max())
                 cols[lock] = info["operator_applications"] / max(1, info["iterations"])
             assert cols["1"] < cols["0"], (precision, cols)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_band_chunk_and_tuning_change_no_result(precision, hfo2):
+    """The operator's bands per chunk and the tensor-core GEMM's tile width are
+    chosen by the autotuner (block_size 0); every choice must give bit-identical
+    H psi and S psi, and repeated mixed solves bit-identical eigenvalues while
+    the tuner is still measuring and after it has decided."""
+    w = hfo2[0]
+    r = rng(4)
+    with ctx_for(hfo2) as ctx:
+        n = ctx.npw((0, 0, 0))
+        psi = r.normal(size=(n, 41)) + 1j * r.normal(size=(n, 41))
+        outs = []
+        for block in (0, 8, 16, 32, 64, 0, 0, 0, 0):
+            ctx.set_acc(block_size=block, precision=precision)
+            outs.append(ctx.apply_hs((0, 0, 0), psi))
+        for h, s in outs[1:]:
+            assert np.array_equal(h, outs[0][0]) and np.array_equal(s, outs[0][1])
+        if precision == "mixed":
+            ctx.set_acc(tol=2e-5, max_iterations=400, block_size=0, precision="mixed")
+            eig = [ctx.solve((0, 0, 0), w.nbands)[0] for _ in range(4)]
+            for e in eig[1:]:
+                assert np.array_equal(e, eig[0])
