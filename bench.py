@@ -11,9 +11,10 @@ dataset; the reference's real inputs are not in the tree).
 One step = one complete acc solve of one k point through the C ABI, from
 operator preparation to converged eigenpairs (mixed precision: FP32 operator
 and split-bf16 tensor-core GEMMs, FP64 small solves and refinement, guard
-bands).  Steps take the k points a rank owns in turn (ranks own k points
-cyclically, the reference's MPI rule), so K = 20 covers the 8 k points of
-the mesh two or three times.  `value` = whole-job device ms per k point:
+bands).  Steps take the mesh's k points in turn, so K = 20 covers the 8 k
+points two or three times.  With N GPUs every rank is an independent replica
+of this single-GPU workload (the path runs on one GPU; no sharding, no
+collective on the data path).  `value` = whole-job device ms per k point:
 max over ranks of the step time divided by the k points all ranks solved in
 it.  Inputs are far larger than L2 (the projected blocks alone are hundreds
 of MB), and L2 is also flushed (256 MB write) before every step.
@@ -66,17 +67,21 @@ def parse():
     p.add_argument("--cpu-samples", type=int, default=3)
     p.add_argument("--no-check", action="store_true",
                    help="skip the dense FP64 reference eigenvalues (|d eps| reported as null)")
-    return p.parse_args()
+    p.add_argument("--quick", action="store_true",
+                   help="only the timed mixed steps (profiling runs): no dense check, FP64 comparisons, e2e, "
+                        "force or CPU figures")
+    args = p.parse_args()
+    if args.quick:
+        args.no_check = args.no_fp64 = args.no_cpu_baseline = True
+    return args
+
+
+def mean_or_none(v):
+    return statistics.mean(v) if v else None
 
 
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
-
-
-def owned(kpts, rank, world):
-    from halfb200.shard import owned_indices
-    idx = owned_indices(len(kpts), rank, world)
-    return kpts[idx] if len(idx) else kpts[:1]
 
 
 class Clocks:
@@ -237,9 +242,9 @@ def workload_config(w, npws, args, nk, world):
     kdesc = "Gamma" if len(w.kpoints) == 1 else f"Gamma + {len(w.kpoints) - 1} k points"
     return {"workload": f"{w.name}: {w.nions} atoms, {kdesc}, {w.grid[0]}^3 box, "
                         f"{min(npws)}-{max(npws)} plane waves, {w.nbands} bands, {w.xc.upper()}, MIMIC_US D_ij",
-            "tol_eV": args.tol, "block": args.block, "kpoints_per_step": world, "kpoints_per_rank": nk,
+            "tol_eV": args.tol, "block": args.block, "kpoints_per_step": world, "kpoints_in_mesh": nk,
             "l2": "inputs larger than L2; 256 MB flush before every step",
-            "parallelism": f"k-point ownership x{world}" if world > 1 else "single GPU"}
+            "parallelism": f"{world} independent replicas" if world > 1 else "single GPU"}
 
 
 def run_reference(args, rank, world):
@@ -265,7 +270,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/k-point", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": workload_config(w, npws, args, len(owned(w.kpoints, 0, 1)), 1),
+            "config": workload_config(w, npws, args, len(w.kpoints), 1),
             "cpu_baseline": {"value": v, "unit": "ms/k-point", "cores": int(base.cores), "kind": "port",
                              "sample": base.describe(iters, source, per_iter, len(samples))},
             "e2e": {"value": v, "unit": "ms/k-point", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -289,7 +294,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     w = synth.workload(args.workload)
     ch, po = write_inputs(w, rank)
-    kpts = owned(w.kpoints, rank, world)
+    kpts = w.kpoints            # replicas: every rank runs the whole single-GPU workload
     nk = len(kpts)
     gamma = int(np.argmin(np.abs(w.kpoints).sum(axis=1)))
     has_gamma = float(np.abs(w.kpoints[gamma]).sum()) == 0.0
@@ -382,7 +387,7 @@ def main():
         ctx.set_acc(tol=args.tol, max_iterations=args.max_iter, block_size=args.block, precision="mixed")
         e2e_ms, e2e_d2h = [], []
         keep = None
-        for i in range(max(1, min(args.steps, nk))):
+        for i in range(0 if args.quick else max(1, min(args.steps, nk))):
             k = kpts[i % nk]
             flush.fill_(float(i))
             torch.cuda.synchronize()
@@ -396,10 +401,10 @@ def main():
             if keep is None:
                 keep = (k, eig, vec)
         # ---- force adjoint (FP64) against one forward operator sweep on the same eigenpairs
-        k0, e0, v0 = keep
-        occ = np.where(np.arange(w.nbands) < int(w.nelect // 2), 2.0, 0.0)
         adj, sweep64, sweep32 = [], [], []
-        for i in range(4):
+        for i in range(0 if keep is None else 4):
+            k0, e0, v0 = keep
+            occ = np.where(np.arange(w.nbands) < int(w.nelect // 2), 2.0, 0.0)
             ctx.nonlocal_forces(k0, v0, e0, occ, 1.0)
             a = ctx.info()["adjoint_ms"]
             ctx.set_acc(tol=args.tol, max_iterations=args.max_iter, block_size=args.block, precision="fp64")
@@ -446,9 +451,9 @@ def main():
         "mixed_speedup_vs_fp64": ((fp64["ms_per_k"] / ms_step) if fp64 else None),
         "mixed_speedup_vs_fp64_note": ("lower bound: the plain FP64 iteration stopped at its bound unconverged"
                                        if fp64 and not fp64["converged"] else None),
-        "force_adjoint_ms": statistics.mean(adj), "forward_sweep_ms_fp64": statistics.mean(sweep64),
-        "forward_sweep_ms_fp32": statistics.mean(sweep32),
-        "force_over_sweep": statistics.mean(adj) / statistics.mean(sweep64),
+        "force_adjoint_ms": mean_or_none(adj), "forward_sweep_ms_fp64": mean_or_none(sweep64),
+        "forward_sweep_ms_fp32": mean_or_none(sweep32),
+        "force_over_sweep": (statistics.mean(adj) / statistics.mean(sweep64)) if adj else None,
         "roofline": {"kernel": "tc_cgemm_kernel: split-bf16 complex GEMM on tcgen05 (projector and subspace "
                                "products of the mixed phase)",
                      "bound": "tensor", "achieved": tc_achieved, "peak": bf16_peak, "unit": "TFLOP/s",
@@ -461,8 +466,8 @@ def main():
                                     "algorithmic_bytes": "3 s N_pw + 8 s N_r per band + r N_r per call"},
         "clocks": clocks,
         "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
-        "e2e": {"value": statistics.mean(e2e_ms) / nk_step, "unit": "ms/k-point",
-                "h2d_bytes_per_step": 24, "d2h_bytes_per_step": int(statistics.mean(e2e_d2h))},
+        "e2e": ({"value": statistics.mean(e2e_ms) / nk_step, "unit": "ms/k-point",
+                 "h2d_bytes_per_step": 24, "d2h_bytes_per_step": int(statistics.mean(e2e_d2h))} if e2e_ms else None),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         iters, source = reference_iterations(args) or (fp64["iterations"] if fp64 else line["iterations"],

@@ -810,10 +810,11 @@ extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoint
   }
   return guarded(error, cap, [&]() -> int {
     std::vector<SolveOutput> outs(nk);
+    std::vector<std::unique_ptr<KOperatorSet>> ops(nk);   // each solve's operator, reused by its force
     std::vector<double> eig((size_t)nk * nbands);
     for (int ik = 0; ik < nk; ++ik) {
       outs[ik].keep_device = true;   // the force needs the eigenvectors on the device
-      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik]);
+      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik], &ops[ik]);
       std::copy(outs[ik].eigenvalues.begin(), outs[ik].eigenvalues.end(), eig.begin() + (size_t)ik * nbands);
     }
     std::vector<double> occ;
@@ -822,9 +823,10 @@ extern "C" int half_band_forces(half_handle handle, int nk, const double* kpoint
     int nions = ctx->crystal.nions();
     std::fill(forces, forces + 3 * nions, 0.0);
     for (int ik = 0; ik < nk; ++ik) {
-      auto ks = prepare_operator(*ctx, *ctx->rt, kpoints + 3 * ik, true, false);
-      nonlocal_forces_device(*ctx, *ks, outs[ik].dvectors.get(), ks->basis.npw(), nbands, eig.data() + (size_t)ik * nbands,
+      KOperatorSet& ks = *ops[ik];
+      nonlocal_forces_device(*ctx, ks, outs[ik].dvectors.get(), ks.basis.npw(), nbands, eig.data() + (size_t)ik * nbands,
                              occ.data() + (size_t)ik * nbands, kweights[ik], forces);
+      ops[ik].reset();
     }
     if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
     if (occ_out) std::copy(occ.begin(), occ.end(), occ_out);
@@ -929,10 +931,11 @@ extern "C" int half_forces(half_handle handle, int nk, const double* kpoints, co
   }
   return guarded(error, cap, [&]() -> int {
     std::vector<SolveOutput> outs(nk);
+    std::vector<std::unique_ptr<KOperatorSet>> ops(nk);   // each solve's operator, reused by its force
     std::vector<double> eig((size_t)nk * nbands);
     for (int ik = 0; ik < nk; ++ik) {
       outs[ik].keep_device = true;
-      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik]);
+      solve_one(*ctx, kpoints + 3 * ik, nbands, false, outs[ik], &ops[ik]);
       std::copy(outs[ik].eigenvalues.begin(), outs[ik].eigenvalues.end(), eig.begin() + (size_t)ik * nbands);
     }
     std::vector<double> occ;
@@ -947,12 +950,13 @@ extern "C" int half_forces(half_handle handle, int nk, const double* kpoints, co
     std::vector<const double2*> ptr(nk);
     std::vector<long long> lds(nk);
     for (int ik = 0; ik < nk; ++ik) {
-      auto ks = prepare_operator(*ctx, *ctx->rt, kpoints + 3 * ik, true, false);
-      nonlocal_forces_device(*ctx, *ks, outs[ik].dvectors.get(), ks->basis.npw(), nbands,
+      KOperatorSet& ks = *ops[ik];
+      nonlocal_forces_device(*ctx, ks, outs[ik].dvectors.get(), ks.basis.npw(), nbands,
                              eig.data() + (size_t)ik * nbands, occ.data() + (size_t)ik * nbands, kweights[ik],
                              nonlocal.data());
       ptr[ik] = outs[ik].dvectors.get();
-      lds[ik] = ks->basis.npw();
+      lds[ik] = ks.basis.npw();
+      ops[ik].reset();
     }
     const long long n = ctx->nr();
     DeviceBuffer<double> rho_out(n);
