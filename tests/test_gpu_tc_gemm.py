@@ -43,8 +43,8 @@ def _run(op_a, op_b, m, n, k, lda_pad=0, ldb_pad=0, ldc_pad=0, alpha=1.0 + 0j, b
     cdt = np.complex128 if c_fp64 else np.complex64
     c0 = c0.astype(cdt)
     da, db, dc = _dev(a, np.complex64), _dev(b, np.complex64), _dev(c0, cdt)
-    halfb200.tc_cgemm(op_a, op_b, m, n, k, alpha, da.data_ptr(), ar + lda_pad, db.data_ptr(), br + ldb_pad, beta,
-                      dc.data_ptr(), m + ldc_pad, c_fp64)
+    halfb200.tc_cgemm(op_a, op_b, m, n, k, alpha, da.data_ptr(), max(1, ar + lda_pad), db.data_ptr(),
+                      max(1, br + ldb_pad), beta, dc.data_ptr(), m + ldc_pad, c_fp64)
     torch.cuda.synchronize()
     got = dc.cpu().numpy()[:m]
     A = _op(a[:ar].astype(np.complex128), op_a)
