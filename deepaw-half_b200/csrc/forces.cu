@@ -1,40 +1,37 @@
-// Hellmann-Feynman band-energy (non-local PAW) force on the GPU.
+// Hellmann-Feynman band-energy (non-local PAW) force on the GPU: a
+// hand-written FP64 adjoint kernel.
 //
 // Reference: add_nonlocal_paw_forces (src/half_forces.F90:9-73), a host triple
 // loop recomputing c = B_I^H psi_n and dc_alpha = B_I^H (i q_alpha psi_n) per
 // atom and band, then
 //   F_I,alpha -= 2 w f_n Re[((D_I - eps_n Q) c)^H dc_alpha] + w f_n Re[c^H dD_I/dR_alpha c].
-// Here all c and dc for all atoms and bands come from ONE GEMM
-//   B^H [psi | i q_x psi | i q_y psi | i q_z psi]   (N_p x 4m, K = N_pw),
-// followed by an epilogue kernel (one block per atom, threads over bands,
-// deterministic tree reduction).  Bands with zero occupation are skipped as
-// in the reference.
+//
+// B200 design: one kernel, one CTA per (atom, 32-band tile), 8 warps.  Per
+// chunk of 32 plane waves the CTA stages psi (coalesced along g), the plane
+// waves' q vectors, the atom's phase exp(+i q.R) (from the packed G indices and
+// the atom's b_j.R / 2 pi, reduced to one turn in FP64) and the chunk of
+// conj(B) = Omega^-1/2 beta_l(|q|) Y_lm(q^) i^l exp(+i q.R) generated from the
+// k point's radial-angular table: B is never stored, and neither is the
+// [psi | i q psi] block.  Lane = band, warp = a group of projector channels:
+// every thread accumulates c and u_alpha = sum_g q_alpha conj(B) psi in FP64
+// registers (dc_alpha = i u_alpha).  The epilogue contracts them with D, Q and
+// dD/dR per band and reduces the 32 bands with warp shuffles; a second kernel
+// adds the band tiles of each atom in order, so the result does not depend on
+// scheduling.  Bands with zero occupation are skipped as in the reference.
 #include <algorithm>
 
-#include "blas.h"
 #include "context.h"
 
 namespace hb {
 
-const double2* projector_matrix64(KOperatorSet& ks);
-
 namespace {
 
 constexpr int kMaxNlm = 32;
-
-__global__ void build_qpsi_kernel(const double2* __restrict__ psi, long long ld, int npw, int nb,
-                                  const double* __restrict__ q, double2* __restrict__ w) {
-  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)npw * nb) return;
-  int b = int(t / npw), g = int(t - (long long)b * npw);
-  double2 x = psi[(long long)b * ld + g];
-  const long long blk = (long long)npw * nb;
-  w[(long long)b * npw + g] = x;
-  for (int a = 0; a < 3; ++a) {
-    double qa = q[3 * g + a];
-    w[(a + 1) * blk + (long long)b * npw + g] = make_double2(-qa * x.y, qa * x.x);   // i q_alpha psi
-  }
-}
+constexpr int kAdjBands = 32;                  // bands per CTA (the lanes)
+constexpr int kAdjGroups = 8;                  // projector-channel groups (the warps)
+constexpr int kAdjG = 32;                      // plane waves per shared-memory chunk
+constexpr int kPerThread = kMaxNlm / kAdjGroups;
+constexpr int kAdjThreads = kAdjBands * kAdjGroups;
 
 struct AtomInfo {
   int col;     // first projector column of the atom
@@ -44,60 +41,173 @@ struct AtomInfo {
   int qofs;    // offset of the species Q
 };
 
-__global__ void force_epilogue_kernel(const double2* __restrict__ cc, int np, int nb, const AtomInfo* __restrict__ atoms,
-                                      const double* __restrict__ dall, const double* __restrict__ ddall,
-                                      const double* __restrict__ qall, const double* __restrict__ eig,
-                                      const double* __restrict__ occ, double kweight, double* __restrict__ out) {
-  const int ion = blockIdx.x;
+size_t adjoint_smem() {
+  const size_t chunk = (size_t(kAdjG) * kMaxNlm + size_t(kAdjG) * kAdjBands) * sizeof(double2) +
+                       size_t(kAdjG) * 4 * sizeof(double);
+  const size_t epilogue = size_t(4) * kAdjBands * kMaxNlm * sizeof(double2);
+  return std::max(chunk, epilogue);
+}
+
+__global__ void __launch_bounds__(kAdjThreads)
+    force_adjoint_kernel(const double2* __restrict__ psi, long long ld, int npw, int nb, const double* __restrict__ qv,
+                         const double* __restrict__ ftab, const int* __restrict__ gpack, const int* __restrict__ pcol,
+                         const double* __restrict__ afrac, double kf0, double kf1, double kf2,
+                         const AtomInfo* __restrict__ atoms, const double* __restrict__ dall,
+                         const double* __restrict__ ddall, const double* __restrict__ qall,
+                         const double* __restrict__ eig, const double* __restrict__ occ, double kweight,
+                         double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* sB = reinterpret_cast<double2*>(smem_raw);      // [kAdjG][kMaxNlm]  conj(B)
+  double2* spsi = sB + kAdjG * kMaxNlm;                     // [kAdjG][kAdjBands]
+  double* sq = reinterpret_cast<double*>(spsi + kAdjG * kAdjBands);   // [kAdjG][4]: q_x, q_y, q_z
+  __shared__ double2 sph[kAdjG];
+  __shared__ int sfrow[kMaxNlm], sl[kMaxNlm];
+  const int ion = blockIdx.x, bt = blockIdx.y;
   const AtomInfo A = atoms[ion];
   const int nlm = A.nlm;
-  const double* D = dall + A.dofs;
-  const double* Q = qall + A.qofs;
-  double f[3] = {0, 0, 0};
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    double fo = occ[b];
-    if (fo == 0.0) continue;
-    double e = eig[b];
-    double2 c[kMaxNlm];
-    for (int a = 0; a < nlm; ++a) c[a] = cc[(long long)b * np + A.col + a];
+  const int tid = threadIdx.x, nl = tid & 31, grp = tid >> 5;
+  const int n = bt * kAdjBands + nl;
+  if (tid < nlm) {
+    const int d = pcol[A.col + tid];
+    sfrow[tid] = (d >> 2) & 0x3FFF;
+    sl[tid] = d & 3;
+  }
+  const int atom = pcol[A.col] >> 16;
+  const double f0 = afrac[3 * atom], f1 = afrac[3 * atom + 1], f2 = afrac[3 * atom + 2];
+  double2 acc[4][kPerThread];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int j = 0; j < kPerThread; ++j) acc[q][j] = make_double2(0.0, 0.0);
+
+  for (int g0 = 0; g0 < npw; g0 += kAdjG) {
+    __syncthreads();   // the previous chunk has been consumed
+    if (tid < kAdjG) {
+      const int g = g0 + tid;
+      double2 ph = make_double2(0.0, 0.0);
+      if (g < npw) {
+        const int gp = gpack[g];
+        const double t = (double((gp << 22) >> 22) + kf0) * f0 + (double((gp << 12) >> 22) + kf1) * f1 +
+                         (double((gp << 2) >> 22) + kf2) * f2;
+        double s, c;
+        sincospi(2.0 * (t - rint(t)), &s, &c);
+        ph = make_double2(c, s);   // exp(+i q.R)
+      }
+      sph[tid] = ph;
+    }
+    for (int t = tid; t < kAdjG * kAdjBands; t += kAdjThreads) {
+      const int gl = t % kAdjG, b = t / kAdjG, g = g0 + gl, nn = bt * kAdjBands + b;
+      spsi[gl * kAdjBands + b] = (g < npw && nn < nb) ? psi[(long long)nn * ld + g] : make_double2(0.0, 0.0);
+    }
+    for (int t = tid; t < kAdjG * 3; t += kAdjThreads) {
+      const int gl = t / 3, a = t - 3 * gl, g = g0 + gl;
+      sq[4 * gl + a] = g < npw ? qv[3 * (long long)g + a] : 0.0;
+    }
+    __syncthreads();
+    for (int t = tid; t < kAdjG * nlm; t += kAdjThreads) {
+      const int gl = t / nlm, a = t - gl * nlm, g = g0 + gl;
+      double2 v = make_double2(0.0, 0.0);
+      if (g < npw) {
+        const double f = ftab[(long long)sfrow[a] * npw + g];
+        const double2 p = sph[gl];
+        double re, im;   // i^l (c + i s)
+        switch (sl[a]) {
+          case 0: re = p.x; im = p.y; break;
+          case 1: re = -p.y; im = p.x; break;
+          case 2: re = -p.x; im = -p.y; break;
+          default: re = p.y; im = -p.x; break;
+        }
+        v = make_double2(f * re, f * im);
+      }
+      sB[gl * kMaxNlm + a] = v;
+    }
+    __syncthreads();
+    if (n < nb) {
+      for (int gl = 0; gl < kAdjG; ++gl) {
+        const double2 x = spsi[gl * kAdjBands + nl];
+        const double qx = sq[4 * gl], qy = sq[4 * gl + 1], qz = sq[4 * gl + 2];
+#pragma unroll
+        for (int j = 0; j < kPerThread; ++j) {
+          const int a = grp + j * kAdjGroups;
+          if (a < nlm) {
+            const double2 b = sB[gl * kMaxNlm + a];
+            const double tr = b.x * x.x - b.y * x.y, ti = b.x * x.y + b.y * x.x;
+            acc[0][j].x += tr;
+            acc[0][j].y += ti;
+            acc[1][j].x = fma(qx, tr, acc[1][j].x);
+            acc[1][j].y = fma(qx, ti, acc[1][j].y);
+            acc[2][j].x = fma(qy, tr, acc[2][j].x);
+            acc[2][j].y = fma(qy, ti, acc[2][j].y);
+            acc[3][j].x = fma(qz, tr, acc[3][j].x);
+            acc[3][j].y = fma(qz, ti, acc[3][j].y);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // c and dc_alpha = i u_alpha of every band of the tile -> shared memory
+  double2* sc = reinterpret_cast<double2*>(smem_raw);   // [4][kAdjBands][kMaxNlm]
+#pragma unroll
+  for (int j = 0; j < kPerThread; ++j) {
+    const int a = grp + j * kAdjGroups;
+    if (a < nlm) {
+      sc[(0 * kAdjBands + nl) * kMaxNlm + a] = acc[0][j];
+      for (int al = 0; al < 3; ++al)
+        sc[((1 + al) * kAdjBands + nl) * kMaxNlm + a] = make_double2(-acc[1 + al][j].y, acc[1 + al][j].x);
+    }
+  }
+  __syncthreads();
+  if (tid >= 32) return;
+  double fsum[3] = {0.0, 0.0, 0.0};
+  const double fo = n < nb ? occ[n] : 0.0;
+  if (fo != 0.0) {
+    const double e = eig[n];
+    const double* D = dall + A.dofs;
+    const double* Q = qall + A.qofs;
+    const double2* c = sc + nl * kMaxNlm;
     double2 mc[kMaxNlm];
     for (int a = 0; a < nlm; ++a) {
-      double2 acc = make_double2(0, 0);
+      double2 s = make_double2(0.0, 0.0);
       for (int k = 0; k < nlm; ++k) {
-        double w = D[a * nlm + k] - e * Q[a * nlm + k];
-        acc.x += w * c[k].x;
-        acc.y += w * c[k].y;
+        const double w = D[a * nlm + k] - e * Q[a * nlm + k];
+        s.x += w * c[k].x;
+        s.y += w * c[k].y;
       }
-      mc[a] = acc;
+      mc[a] = s;
     }
     for (int al = 0; al < 3; ++al) {
-      const double2* dc = cc + (long long)(al + 1) * nb * np + (long long)b * np + A.col;
-      double re = 0;
+      const double2* dc = sc + ((1 + al) * kAdjBands + nl) * kMaxNlm;
+      double re = 0.0;
       for (int a = 0; a < nlm; ++a) re += mc[a].x * dc[a].x + mc[a].y * dc[a].y;   // Re(conj(mc) . dc)
-      double t1 = -2.0 * kweight * fo * re;
       const double* dD = ddall + A.ddofs + al * nlm * nlm;
-      double q = 0;
+      double q = 0.0;
       for (int a = 0; a < nlm; ++a) {
-        double2 acc = make_double2(0, 0);
+        double2 s = make_double2(0.0, 0.0);
         for (int k = 0; k < nlm; ++k) {
-          acc.x += dD[a * nlm + k] * c[k].x;
-          acc.y += dD[a * nlm + k] * c[k].y;
+          s.x += dD[a * nlm + k] * c[k].x;
+          s.y += dD[a * nlm + k] * c[k].y;
         }
-        q += c[a].x * acc.x + c[a].y * acc.y;   // Re(conj(c) . dD c)
+        q += c[a].x * s.x + c[a].y * s.y;   // Re(conj(c) . dD c)
       }
-      f[al] += t1 - kweight * fo * q;
+      fsum[al] = -2.0 * kweight * fo * re - kweight * fo * q;
     }
   }
-  __shared__ double red[3][256];
-  for (int al = 0; al < 3; ++al) red[al][threadIdx.x] = f[al];
-  __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      for (int al = 0; al < 3; ++al) red[al][threadIdx.x] += red[al][threadIdx.x + w];
-    __syncthreads();
+  for (int al = 0; al < 3; ++al) {
+    double v = fsum[al];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (tid == 0) partial[((long long)ion * gridDim.y + bt) * 3 + al] = v;
   }
-  if (threadIdx.x == 0)
-    for (int al = 0; al < 3; ++al) out[3 * ion + al] = red[al][0];
+}
+
+// out[ion][alpha] = sum over band tiles, in tile order.
+__global__ void sum_tiles_kernel(const double* __restrict__ partial, int nions, int ntiles, double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nions * 3) return;
+  const int ion = t / 3, al = t - 3 * ion;
+  double s = 0.0;
+  for (int b = 0; b < ntiles; ++b) s += partial[((long long)ion * ntiles + b) * 3 + al];
+  out[t] = s;
 }
 
 }  // namespace
@@ -130,24 +240,25 @@ void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec,
     ddall.insert(ddall.end(), ddh.begin(), ddh.end());
     col0 += sp.natoms * sp.nlm;
   }
+  const int ntiles = (nb + kAdjBands - 1) / kAdjBands;
   DeviceBuffer<AtomInfo> datoms;
   datoms.upload(atoms, st);
-  DeviceBuffer<double> dd, ddd, dq, deig, docc, dout(size_t(nions) * 3);
+  DeviceBuffer<double> dd, ddd, dq, deig, docc, dpart(size_t(nions) * ntiles * 3), dout(size_t(nions) * 3);
   dd.upload(dall, st);
   ddd.upload(ddall, st);
   dq.upload(qall, st);
   deig.upload(eig, nb, st);
   docc.upload(occ, nb, st);
-  DeviceBuffer<double2> w(size_t(4) * npw * nb), cc(size_t(4) * np * nb);
+  const size_t smem = adjoint_smem();
+  raise_smem_limit(force_adjoint_kernel, smem);
   Profile& pf = rt.prof;
   const int ev0 = pf.record(st);
-  build_qpsi_kernel<<<ceil_div((long long)npw * nb, 256), 256, 0, st>>>(dvec, ld, npw, nb, ks.qvec.get(), w.get());
-  HALF_LAUNCH("force qpsi");
-  const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
-  gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, 4 * nb, npw, one, projector_matrix64(ks), npw, w.get(), npw, zero, cc.get(), np);
-  force_epilogue_kernel<<<nions, 256, 0, st>>>(cc.get(), np, nb, datoms.get(), dd.get(), ddd.get(), dq.get(), deig.get(),
-                                               docc.get(), kweight, dout.get());
-  HALF_LAUNCH("force epilogue");
+  force_adjoint_kernel<<<dim3(nions, ntiles), kAdjThreads, smem, st>>>(
+      dvec, ld, npw, nb, ks.qvec.get(), ks.ftab64.get(), ks.gpack.get(), ks.pcol.get(), ks.afrac.get(), ks.kf[0],
+      ks.kf[1], ks.kf[2], datoms.get(), dd.get(), ddd.get(), dq.get(), deig.get(), docc.get(), kweight, dpart.get());
+  HALF_LAUNCH("force adjoint");
+  sum_tiles_kernel<<<ceil_div(nions * 3, 128), 128, 0, st>>>(dpart.get(), nions, ntiles, dout.get());
+  HALF_LAUNCH("force tiles");
   pf.span(Profile::kAdjoint, ev0, pf.record(st));
   pf.launches += 2;
   auto f = dout.download(st);

@@ -291,13 +291,13 @@ __global__ void projector_kernel(double2* __restrict__ B, int npw, const double*
 
 // ftab[r][g] = Omega^-1/2 beta_l(|q|) Y_lm(q^) for the channel rows of the
 // generated FP32 projector tiles (one row per (species, channel, m)).
-__global__ void radial_angular_table_kernel(float* __restrict__ ftab, int npw, const double* __restrict__ q,
+__global__ void radial_angular_table_kernel(double* __restrict__ ftab, int npw, const double* __restrict__ q,
                                             const ProjCol* __restrict__ rows, const double* __restrict__ ry,
                                             const double* __restrict__ rm2, double pref) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   int r = blockIdx.y;
   if (g >= npw) return;
-  ftab[(long long)r * npw + g] = float(pref * radial_angular(rows[r], q[3 * g], q[3 * g + 1], q[3 * g + 2], ry, rm2));
+  ftab[(long long)r * npw + g] = pref * radial_angular(rows[r], q[3 * g], q[3 * g + 1], q[3 * g + 2], ry, rm2);
 }
 
 template <typename R>
@@ -356,8 +356,9 @@ HostGeom plane_geometry(const Basis& b, const AxisPlan& ax, const AxisPlan& ay, 
 // row per (species, channel, m), the column descriptors, and the ions' b_j.R / 2 pi.
 struct ProjGen {
   std::vector<ProjCol> frows;
-  std::vector<int> pcol;
+  std::vector<int> pcol, gpack;
   std::vector<double> afrac;
+  const double* ftab64 = nullptr;   // device [frow][npw], built by prepare_operator
   const double* qvec = nullptr;   // device npw x 3
   const double* ry = nullptr;     // device radial tables
   const double* rm2 = nullptr;
@@ -392,21 +393,14 @@ void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom
     op.B.resize(B64.size());
     HALF_CUDA(cudaMemcpyAsync(op.B.get(), B64.get(), B64.size() * sizeof(double2), cudaMemcpyDeviceToDevice, s));
   } else if (np > 0) {
-    const int npw = int(basis.npw()), nf = int(gen.frows.size());
-    DeviceBuffer<ProjCol> drows;
-    drows.upload(gen.frows, s);
-    op.ftab.resize(size_t(nf) * npw);
-    radial_angular_table_kernel<<<dim3(ceil_div(npw, 256), nf), 256, 0, s>>>(op.ftab.get(), npw, gen.qvec, drows.get(),
-                                                                            gen.ry, gen.rm2, gen.pref);
-    HALF_LAUNCH("radial-angular table");
-    std::vector<int> gp(npw);
-    for (int g = 0; g < npw; ++g)
-      gp[g] = (basis.gvec[3 * g] & 1023) | ((basis.gvec[3 * g + 1] & 1023) << 10) | ((basis.gvec[3 * g + 2] & 1023) << 20);
-    op.gpack.upload(gp, s);
+    const long long nt = (long long)gen.frows.size() * basis.npw();
+    op.ftab.resize(size_t(nt));
+    scale_copy_kernel<float><<<ceil_div(nt, 256), 256, 0, s>>>(gen.ftab64, op.ftab.get(), nt, 1.0);
+    HALF_LAUNCH("radial-angular table (FP32)");
+    op.gpack.upload(gen.gpack, s);
     op.pcol.upload(gen.pcol, s);
     op.afrac.upload(gen.afrac, s);
     for (int j = 0; j < 3; ++j) op.kf[j] = basis.kpoint[j];
-    HALF_CUDA(cudaStreamSynchronize(s));   // drows is released on return
   }
   std::vector<double> dall, qall;
   for (auto& sp : ctx.species) {
@@ -517,6 +511,24 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
   gen.ry = dry.get();
   gen.rm2 = drm2.get();
   gen.pref = 1.0 / std::sqrt(ctx.crystal.volume());
+  DeviceBuffer<ProjCol> drows;
+  if (np > 0) {   // in-tile generation tables, shared by the FP32 operator and the force adjoint
+    const int nf = int(gen.frows.size());
+    drows.upload(gen.frows, s);
+    ks->ftab64.resize(size_t(nf) * npw);
+    radial_angular_table_kernel<<<dim3(ceil_div(npw, 256), nf), 256, 0, s>>>(ks->ftab64.get(), npw, ks->qvec.get(),
+                                                                            drows.get(), dry.get(), drm2.get(), gen.pref);
+    HALF_LAUNCH("radial-angular table");
+    gen.gpack.resize(npw);
+    for (int g = 0; g < npw; ++g)
+      gen.gpack[g] = (basis.gvec[3 * g] & 1023) | ((basis.gvec[3 * g + 1] & 1023) << 10) |
+                     ((basis.gvec[3 * g + 2] & 1023) << 20);
+    ks->gpack.upload(gen.gpack, s);
+    ks->pcol.upload(gen.pcol, s);
+    ks->afrac.upload(gen.afrac, s);
+    for (int j = 0; j < 3; ++j) ks->kf[j] = basis.kpoint[j];
+    gen.ftab64 = ks->ftab64.get();
+  }
   if (np > 0) {
     projector_kernel<<<dim3(ceil_div(npw, 256), np), 256, 0, s>>>(B64.get(), npw, ks->qvec.get(), dcols.get(), dry.get(),
                                                                    drm2.get(), dpos.get(), 1.0 / std::sqrt(ctx.crystal.volume()));
