@@ -73,11 +73,14 @@ struct Out {
   int M, N;
 };
 
-__device__ __forceinline__ void split2(float x, uint32_t& hi, uint32_t& lo) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-  hi = __bfloat16_as_ushort(h);
-  lo = __bfloat16_as_ushort(l);
+// Two values at once (packed cvt.rn.bf16x2.f32): hi = (bf16(a), bf16(b)),
+// lo = (bf16(a - hi.a), bf16(b - hi.b)), first value in the low half.
+__device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 // Splits this lane's element and stores, with its neighbour (lane ^ 1), one
@@ -85,11 +88,9 @@ __device__ __forceinline__ void split2(float x, uint32_t& hi, uint32_t& lo) {
 // The pair's first element is the even lane's.  Every lane must call this.
 __device__ __forceinline__ void store_pair(float2 v, int lane, uint32_t base, uint32_t pstride, uint32_t off,
                                            bool store) {
-  uint32_t rh, rl, ih, il;
-  split2(v.x, rh, rl);
-  split2(v.y, ih, il);
+  uint32_t hi, lo;   // (Re, Im) hi parts and lo parts
+  split_pair(v.x, v.y, hi, lo);
   const bool even = (lane & 1) == 0;
-  const uint32_t hi = rh | (ih << 16), lo = rl | (il << 16);
   const uint32_t recv = __shfl_xor_sync(0xffffffffu, even ? lo : hi, 1);
   const uint32_t own = even ? hi : lo;
   const uint32_t a = even ? own : recv, b = even ? recv : own;
@@ -181,15 +182,8 @@ __device__ __forceinline__ void store_chunk8(const float2 (&v)[8], uint32_t base
   uint32_t w[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    uint32_t rh0, rl0, ih0, il0, rh1, rl1, ih1, il1;
-    split2(v[2 * i].x, rh0, rl0);
-    split2(v[2 * i].y, ih0, il0);
-    split2(v[2 * i + 1].x, rh1, rl1);
-    split2(v[2 * i + 1].y, ih1, il1);
-    w[0][i] = rh0 | (rh1 << 16);
-    w[1][i] = rl0 | (rl1 << 16);
-    w[2][i] = ih0 | (ih1 << 16);
-    w[3][i] = il0 | (il1 << 16);
+    split_pair(v[2 * i].x, v[2 * i + 1].x, w[0][i], w[1][i]);
+    split_pair(v[2 * i].y, v[2 * i + 1].y, w[2][i], w[3][i]);
   }
 #pragma unroll
   for (int p = 0; p < 4; ++p) st_shared_v4(base + uint32_t(p) * pstride + off, w[p][0], w[p][1], w[p][2], w[p][3]);
