@@ -67,6 +67,10 @@ def parse():
     p.add_argument("--cpu-samples", type=int, default=3)
     p.add_argument("--no-check", action="store_true",
                    help="skip the dense FP64 reference eigenvalues (|d eps| reported as null)")
+    p.add_argument("--kernel", default=None, choices=["gemm"],
+                   help="micro-benchmark one kernel on the workload's shapes instead of the solve (gemm: the "
+                        "tensor-core complex GEMM on the mixed phase's subspace shapes, synthetic operands)")
+    p.add_argument("--reps", type=int, default=10, help="repetitions per shape of --kernel")
     p.add_argument("--quick", action="store_true",
                    help="only the timed mixed steps (profiling runs): no dense check, FP64 comparisons, e2e, "
                         "force or CPU figures")
@@ -277,11 +281,51 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_gemm_kernel(args):
+    """--kernel gemm: the tensor-core GEMM (half_tc_cgemm) on the mixed phase's
+    subspace shapes of the workload's first k point (m = bands + guard bands),
+    with seeded complex64 operands; wall time per call over --reps calls (each
+    call returns when its result is complete).  Rate = 24 M N K bf16 flops per
+    call against the measured dense bf16 peak."""
+    import halfb200
+    from halfb200 import synth
+    import torch
+    w = synth.workload(args.workload)
+    ch, po = write_inputs(w, 0)
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
+        n = ctx.npw(w.kpoints[0])
+    m = w.nbands + min(max(4, w.nbands // 8), n // 2 - w.nbands)
+    peaks, kind = measured_peaks()
+    g = torch.Generator(device="cuda").manual_seed(1)
+    big = [torch.randn((m, n), dtype=torch.complex64, device="cuda", generator=g) for _ in range(2)]   # n x m column-major
+    small = torch.randn((m, m), dtype=torch.complex64, device="cuda", generator=g)
+    out32 = torch.zeros((m, n), dtype=torch.complex64, device="cuda")
+    out64 = torch.zeros((m, m), dtype=torch.complex128, device="cuda")
+    outsm = torch.zeros((m, m), dtype=torch.complex64, device="cuda")
+    shapes = [("inner X^H Y (m x m, K = N_pw), FP64 output", "C", "N", m, m, n, big[0], n, big[1], n, out64, m, True),
+              ("inner X^H Y (m x m, K = N_pw)", "C", "N", m, m, n, big[0], n, big[1], n, outsm, m, False),
+              ("rotation X Y (N_pw x m, K = m)", "N", "N", n, m, m, big[0], n, small, m, out32, n, False)]
+    for name, oa, ob, M, N, K, a, lda, b, ldb, c, ldc, f64 in shapes:
+        for i in range(args.warmup + args.reps):
+            if i == args.warmup:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+            halfb200.tc_cgemm(oa, ob, M, N, K, 1.0 + 0j, a.data_ptr(), lda, b.data_ptr(), ldb, 0j, c.data_ptr(), ldc, f64)
+        dt = (time.perf_counter() - t0) / max(1, args.reps)
+        tf = 24.0 * M * N * K / dt / 1e12
+        print(json.dumps({"kernel": "tc_cgemm_kernel", "shape": name, "M": M, "N": N, "K": K, "ms": dt * 1e3,
+                          "tflops_bf16": tf, "peak": peaks.get("bf16_tflops"), "frac": tf / peaks["bf16_tflops"],
+                          "peak_source": kind, "workload": w.name}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.kernel == "gemm":
+        run_gemm_kernel(args)
         return
     import halfb200
     from halfb200 import synth

@@ -483,10 +483,12 @@ struct AccRun {
 // Mixed refinement: after the FP32 phase, X, H X and S X are FP64 and are
 // rotated with FP64 GEMMs, while the correction directions P, H P, S P are
 // FP32 (FP32 operator, tensor-core GEMMs against FP32 shadows of X, H X,
-// S X).  The errors of everything built from P are relative to |P|, which
-// falls with the residual, so the iteration converges to FP64 accuracy at
-// the cost of the FP32 iteration plus five FP64 GEMMs of N x m x m (the
-// X-block of each projected matrix and the three rotations by Y_top).  An
+// S X).  The X-P blocks of the Rayleigh-Ritz pencil are formed in FP64 as
+// (H X)^H P and (S X)^H P, so every remaining FP32 error enters the new X and
+// H X multiplied by the Ritz vectors' P coefficients, which fall with the
+// residual: the iteration converges to FP64 accuracy at the cost of the FP32
+// iteration plus seven FP64 GEMMs of N x m x m (four projected blocks and the
+// three rotations by Y_top).  An
 // exact FP64 operator sweep on X confirms convergence before the solve
 // returns (the north star's final FP64 residual sweep).
 struct Refine {
@@ -539,17 +541,25 @@ struct Refine {
     float2* hpu = skip_metric ? F.HP.get() : F.HPU.get();
     float2* spu = skip_metric ? F.SP.get() : F.SPU.get();
     if (!skip_metric) r32.normalise_metric(one, zero, np);
-    // Rayleigh-Ritz pencil (upper triangle): the X block in FP64, the P blocks
-    // from the tensor-core GEMMs written as FP64
+    // Rayleigh-Ritz pencil (upper triangle).  Near convergence the X-P blocks
+    // X^H H P and X^H S P are as small as the residual while P has unit norm,
+    // so they must not carry errors relative to |P|: they are formed in FP64
+    // as (H X)^H P and (S X)^H P (H and S are Hermitian) from the exact FP64
+    // H X, S X and P widened to FP64.  The X block is FP64 too; only the P
+    // block, whose errors enter the Ritz vectors times their P coefficients,
+    // comes from the tensor cores.
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
     const double2 d1 = make_double2(1, 0), d0 = make_double2(0, 0);
     const int ld = ord;
+    double2* p64 = B.P.get();
+    convert_kernel<float2, double2><<<ceil_div((long long)n * np, 256), 256, 0, rt.stream>>>(pu, p64, (long long)n * np);
+    ++rt.prof.launches;
     gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, d1, B.x(), n, B.hx(), n, d0, hs, ld);
-    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, x32, n, hpu, n, hs + (long long)m * ld, ld);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, d1, B.hx(), n, p64, n, d0, hs + (long long)m * ld, ld);
     gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, pu, n, hpu, n, hs + (long long)m * ld + m, ld);
     gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, d1, B.x(), n, B.sx(), n, d0, ssb, ld);
-    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, x32, n, spu, n, ssb + (long long)m * ld, ld);
+    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, d1, B.sx(), n, p64, n, d0, ssb + (long long)m * ld, ld);
     gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, pu, n, spu, n, ssb + (long long)m * ld + m, ld);
     ss.hegvd(hs, ssb, ord, sc.w.get(), m);
     // rotations: FP64 X Y_top, then + P Y_bot on the tensor cores accumulated in FP64
