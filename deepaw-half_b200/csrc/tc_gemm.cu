@@ -101,14 +101,19 @@ __device__ __forceinline__ void store_pair(float2 v, int lane, uint32_t base, ui
   }
 }
 
-// Dense operand with k contiguous: each warp step covers 4 rows x 8 k.
-__device__ __forceinline__ void fill_dense_k(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                             uint32_t pstride, int warp, int lane) {
+// Dense operands are filled in two halves so the producer loop can issue
+// the global loads of stage i + 1 before it splits and stores stage i:
+// load_dense_* brings this warp's elements of one slice into registers (zero
+// outside the matrix), store_dense_* splits and stores them.  NV is the
+// register count per lane: 8 for the 128-row A slice, 16 for B (up to 256 rows).
+
+// k contiguous: each warp step covers 4 rows x 8 k.
+template <int NV>
+__device__ __forceinline__ void load_dense_k(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
+                                             float2 (&v)[NV]) {
   const int nsteps = (R >> 2) * 2;
-  constexpr int kPer = 16;
-  float2 v[kPer];
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < NV; ++i) {
     const int t = warp + i * kProdWarps;
     v[i] = make_float2(0.f, 0.f);
     if (t < nsteps) {
@@ -119,8 +124,14 @@ __device__ __forceinline__ void fill_dense_k(const TcOperand& op, int r0, int R,
       }
     }
   }
+}
+
+template <int NV>
+__device__ __forceinline__ void store_dense_k(const TcOperand& op, int R, uint32_t base, uint32_t pstride, int warp,
+                                              int lane, const float2 (&v)[NV]) {
+  const int nsteps = (R >> 2) * 2;
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < NV; ++i) {
     const int t = warp + i * kProdWarps;
     if (t < nsteps) {
       const int r = (t >> 1) * 4 + (lane >> 3), kl = (t & 1) * 8 + (lane & 7);
@@ -133,14 +144,13 @@ __device__ __forceinline__ void fill_dense_k(const TcOperand& op, int r0, int R,
   }
 }
 
-// Dense operand with rows contiguous: each warp step covers 32 rows at one k.
-__device__ __forceinline__ void fill_dense_mn(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                              uint32_t pstride, int warp, int lane) {
+// rows contiguous: each warp step covers 32 rows at one k.
+template <int NV>
+__device__ __forceinline__ void load_dense_mn(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
+                                              float2 (&v)[NV]) {
   const int nsteps = ((R + 31) >> 5) * 16;
-  constexpr int kPer = 16;
-  float2 v[kPer];
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < NV; ++i) {
     const int t = warp + i * kProdWarps;
     v[i] = make_float2(0.f, 0.f);
     if (t < nsteps) {
@@ -148,8 +158,14 @@ __device__ __forceinline__ void fill_dense_mn(const TcOperand& op, int r0, int R
       if (rl < R && r < op.rows && k < op.kdim) v[i] = __ldg(op.p + r + (long long)k * op.ld);
     }
   }
+}
+
+template <int NV>
+__device__ __forceinline__ void store_dense_mn(const TcOperand& op, int R, uint32_t base, uint32_t pstride, int warp,
+                                               int lane, const float2 (&v)[NV]) {
+  const int nsteps = ((R + 31) >> 5) * 16;
 #pragma unroll
-  for (int i = 0; i < kPer; ++i) {
+  for (int i = 0; i < NV; ++i) {
     const int t = warp + i * kProdWarps;
     if (t < nsteps) {
       const int rl = (t >> 4) * 32 + lane, kl = t & 15, rp = rl & ~1;
@@ -270,11 +286,21 @@ __device__ __forceinline__ void fill_proj(const TcOperand& op, int r0, int R, in
   }
 }
 
-__device__ __forceinline__ void fill_operand(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                             uint32_t pstride, int warp, int lane) {
+template <int NV>
+__device__ __forceinline__ void load_operand(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
+                                             float2 (&v)[NV]) {
+  if (op.kind == TcOperand::kDenseK) load_dense_k(op, r0, R, k0, warp, lane, v);
+  else if (op.kind == TcOperand::kDenseMN) load_dense_mn(op, r0, R, k0, warp, lane, v);
+}
+
+// Generated operands compute their elements here; dense ones store the
+// registers their load_operand brought in.
+template <int NV>
+__device__ __forceinline__ void store_operand(const TcOperand& op, int r0, int R, int k0, uint32_t base,
+                                              uint32_t pstride, int warp, int lane, const float2 (&v)[NV]) {
   switch (op.kind) {
-    case TcOperand::kDenseK: fill_dense_k(op, r0, R, k0, base, pstride, warp, lane); break;
-    case TcOperand::kDenseMN: fill_dense_mn(op, r0, R, k0, base, pstride, warp, lane); break;
+    case TcOperand::kDenseK: store_dense_k(op, R, base, pstride, warp, lane, v); break;
+    case TcOperand::kDenseMN: store_dense_mn(op, R, base, pstride, warp, lane, v); break;
     case TcOperand::kProjConj: fill_proj_conj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
     default: fill_proj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
   }
@@ -333,16 +359,36 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = tmem_slot;
 
   if (warp < kProdWarps) {
-    for (int i = 0; i < nkb; ++i) {
-      const int s = i % kStages;
-      if (i >= kStages && !__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ((i / kStages) - 1) & 1, abort))) break;
-      const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
-      const int k0 = (kb0 + i) * kBK;
-      fill_operand(A, m0, kBM, k0, abase, a_ps, warp, lane);
-      fill_operand(B, n0, bn, k0, bbase, b_ps, warp, lane);
-      fence_proxy_async_smem();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&full_bar[s]);
+    // software pipeline: the dense loads of stage i + 1 are in flight while
+    // stage i is split and stored
+    float2 va[2][8], vb[2][16];
+    if (nkb > 0) {
+      load_operand(A, m0, kBM, kb0 * kBK, warp, lane, va[0]);
+      load_operand(B, n0, bn, kb0 * kBK, warp, lane, vb[0]);
+    }
+    for (int i = 0; i < nkb; i += 2) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int ii = i + h;
+        if (ii < nkb) {
+          if (ii + 1 < nkb) {
+            load_operand(A, m0, kBM, (kb0 + ii + 1) * kBK, warp, lane, va[h ^ 1]);
+            load_operand(B, n0, bn, (kb0 + ii + 1) * kBK, warp, lane, vb[h ^ 1]);
+          }
+          const int s = ii % kStages;
+          if (ii >= kStages && !__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ((ii / kStages) - 1) & 1, abort))) {
+            i = nkb;   // leave both loops
+            break;
+          }
+          const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
+          const int k0 = (kb0 + ii) * kBK;
+          store_operand(A, m0, kBM, k0, abase, a_ps, warp, lane, va[h]);
+          store_operand(B, n0, bn, k0, bbase, b_ps, warp, lane, vb[h]);
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&full_bar[s]);
+        }
+      }
     }
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, every other 16-column chunk
     if (__all_sync(0xffffffffu, mbar_wait(&accum_bar, 0, abort))) {
