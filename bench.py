@@ -270,7 +270,8 @@ def run_reference(args, rank, world):
             samples.append((base.t_prep + iters * s) * 1e3)
     v = statistics.median(samples)
     per_iter = (v / 1e3 - base.t_prep) / iters
-    npws = [base.npw]
+    from oracle.basis import build_basis
+    npws = [build_basis(base.sysm.crystal, w.grid, w.encut, k).npw for k in w.kpoints]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ms/k-point", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": v, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
