@@ -27,11 +27,9 @@
 //   split-bf16 tcgen05 GEMMs from tc_gemm.cu whose projected matrices land
 //   directly in FP64, FP64 small eigensolves) until the residual reaches the
 //   FP32 regime, then promotes X
-//   and refines it in mixed precision (X, H X, S X in FP64 with FP64
-//   rotations; the corrections through the FP32 operator and tensor-core
-//   GEMMs; an exact FP64 operator sweep before convergence is declared,
-//   struct Refine); it carries m/8 (at least 4) guard bands and tests
-//   convergence on the requested m.
+//   and finishes with FP64 iterations (one FP64 operator sweep re-creates
+//   H X and S X exactly before the first FP64 Rayleigh-Ritz); it carries
+//   m/8 (at least 4) guard bands and tests convergence on the requested m.
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -480,105 +478,6 @@ struct AccRun {
   }
 };
 
-// Mixed refinement: after the FP32 phase, X, H X and S X are FP64 and are
-// rotated with FP64 GEMMs, while the correction directions P, H P, S P are
-// FP32 (FP32 operator, tensor-core GEMMs against FP32 shadows of X, H X,
-// S X).  The X-P blocks of the Rayleigh-Ritz pencil are formed in FP64 as
-// (H X)^H P and (S X)^H P, so every remaining FP32 error enters the new X and
-// H X multiplied by the Ritz vectors' P coefficients, which fall with the
-// residual: the iteration converges to FP64 accuracy at the cost of the FP32
-// iteration plus seven FP64 GEMMs of N x m x m (four projected blocks and the
-// three rotations by Y_top).  An
-// exact FP64 operator sweep on X confirms convergence before the solve
-// returns (the north star's final FP64 residual sweep).
-struct Refine {
-  AccRun<double>& r64;
-  AccRun<float>& r32;   // its X[0], HX[0], SX[0] hold the FP32 shadows
-  Runtime& rt;
-  Scratch64& sc;
-  SmallSolver& ss;
-  int n, m;
-
-  void shadow() {
-    Blocks<double>& B = r64.blk;
-    Blocks<float>& F = r32.blk;
-    F.cur = 0;
-    const long long nm = (long long)n * m;
-    convert_kernel<double2, float2><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(B.x(), F.X[0].get(), nm);
-    convert_kernel<double2, float2><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(B.hx(), F.HX[0].get(), nm);
-    convert_kernel<double2, float2><<<ceil_div(nm, 256), 256, 0, rt.stream>>>(B.sx(), F.SX[0].get(), nm);
-    HALF_LAUNCH("FP32 shadows");
-    rt.prof.launches += 3;
-  }
-
-  void iterate(double seed_threshold, const std::vector<int>* active) {
-    Blocks<double>& B = r64.blk;
-    Blocks<float>& F = r32.blk;
-    const int np = active ? int(active->size()) : m;
-    const int* cols = nullptr;
-    if (np < m) {
-      sc.active.upload(*active, rt.stream);
-      cols = sc.active.get();
-    }
-    const long long nmp = (long long)n * np;
-    precondition_kernel<double2, float2><<<ceil_div(nmp, 256), 256, 0, rt.stream>>>(
-        B.hx(), B.sx(), n, n, m, np, cols, sc.w.get(), sc.norms.get(), seed_threshold, sc.kinetic.get(), F.P.get());
-    ++rt.prof.launches;
-    HALF_LAUNCH("precondition");
-    r32.apply(F.P.get(), F.HP.get(), F.SP.get(), np);
-    const float2 one = cval<float>(1.0), zero = cval<float>(0.0), mone = cval<float>(-1.0);
-    float2* x32 = F.X[0].get();
-    float2* hx32 = F.HX[0].get();
-    float2* sx32 = F.SX[0].get();
-    // S-orthogonalise against X (FP32 shadows)
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, one, x32, n, F.SP.get(), n, zero, F.small.get(), m);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, x32, n, F.small.get(), m, one, F.P.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, hx32, n, F.small.get(), m, one, F.HP.get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, sx32, n, F.small.get(), m, one, F.SP.get(), n);
-    const int ord = m + np;
-    const bool skip_metric = r32.guarded && ss.own && ord <= SmallEigen::kOwnMaxOrder;
-    float2* pu = skip_metric ? F.P.get() : F.PU.get();
-    float2* hpu = skip_metric ? F.HP.get() : F.HPU.get();
-    float2* spu = skip_metric ? F.SP.get() : F.SPU.get();
-    if (!skip_metric) r32.normalise_metric(one, zero, np);
-    // Rayleigh-Ritz pencil (upper triangle).  Near convergence the X-P blocks
-    // X^H H P and X^H S P are as small as the residual while P has unit norm,
-    // so they must not carry errors relative to |P|: they are formed in FP64
-    // as (H X)^H P and (S X)^H P (H and S are Hermitian) from the exact FP64
-    // H X, S X and P widened to FP64.  The X block is FP64 too; only the P
-    // block, whose errors enter the Ritz vectors times their P coefficients,
-    // comes from the tensor cores.
-    double2* hs = sc.hsub.get();
-    double2* ssb = sc.ssub.get();
-    const double2 d1 = make_double2(1, 0), d0 = make_double2(0, 0);
-    const int ld = ord;
-    double2* p64 = B.P.get();
-    convert_kernel<float2, double2><<<ceil_div((long long)n * np, 256), 256, 0, rt.stream>>>(pu, p64, (long long)n * np);
-    ++rt.prof.launches;
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, d1, B.x(), n, B.hx(), n, d0, hs, ld);
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, d1, B.hx(), n, p64, n, d0, hs + (long long)m * ld, ld);
-    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, pu, n, hpu, n, hs + (long long)m * ld + m, ld);
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, m, n, d1, B.x(), n, B.sx(), n, d0, ssb, ld);
-    gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, m, np, n, d1, B.sx(), n, p64, n, d0, ssb + (long long)m * ld, ld);
-    gemm_to64(rt, CUBLAS_OP_C, CUBLAS_OP_N, np, np, n, pu, n, spu, n, ssb + (long long)m * ld + m, ld);
-    ss.hegvd(hs, ssb, ord, sc.w.get(), m);
-    // rotations: FP64 X Y_top, then + P Y_bot on the tensor cores accumulated in FP64
-    convert_block_kernel<double2, float2><<<ceil_div((long long)np * m, 256), 256, 0, rt.stream>>>(
-        hs + m, ld, F.Y.get(), np, np, m);
-    ++rt.prof.launches;
-    const int nx = B.cur ^ 1;
-    const TcOperand yb = tc_dense_b(CUBLAS_OP_N, F.Y.get(), np, np, m);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, d1, B.x(), n, hs, ld, d0, B.X[nx].get(), n);
-    tc_cgemm(rt, tc_dense_a(CUBLAS_OP_N, pu, n, n, np), yb, n, m, np, d1, d1, B.X[nx].get(), true, n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, d1, B.hx(), n, hs, ld, d0, B.HX[nx].get(), n);
-    tc_cgemm(rt, tc_dense_a(CUBLAS_OP_N, hpu, n, n, np), yb, n, m, np, d1, d1, B.HX[nx].get(), true, n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, d1, B.sx(), n, hs, ld, d0, B.SX[nx].get(), n);
-    tc_cgemm(rt, tc_dense_a(CUBLAS_OP_N, spu, n, n, np), yb, n, m, np, d1, d1, B.SX[nx].get(), true, n);
-    B.cur = nx;
-    shadow();
-  }
-};
-
 }  // namespace
 
 void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, SolveOutput& out, SolveInfo& info) {
@@ -681,39 +580,11 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     ++rt.prof.launches;
     run64.apply(b64.x(), b64.hx(), b64.sx(), m);
     run64.rayleigh_ritz_x();
-    // Environment HALF_REFINE=mixed selects the mixed refinement (struct Refine);
-    // otherwise the refinement runs entirely in FP64.
-    const char* rsel = std::getenv("HALF_REFINE");
-    const bool fp64_refine = !(rsel && std::string(rsel) == "mixed");
-    if (fp64_refine) {
-      for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
-        max_res = run64.residuals(norms, infos);
-        tracer.step("fp64", fp64_iter, max_res, norms);
-        if (max_res <= cfg.tol) { converged = true; break; }
-        run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
-      }
-    } else {
-      Refine refine{run64, run32, rt, sc, ss, n, m};
-      refine.shadow();
-      bool exact = true;   // H X and S X are the operator applied to the current X
-      for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
-        max_res = run64.residuals(norms, infos);
-        tc_check(rt);
-        tracer.step("refine", fp64_iter, max_res, norms);
-        if (max_res <= cfg.tol) {
-          if (exact) { converged = true; break; }
-          // the final FP64 sweep: exact H X, S X and their Rayleigh-Ritz
-          run64.apply(b64.x(), b64.hx(), b64.sx(), m);
-          run64.rayleigh_ritz_x();
-          exact = true;
-          max_res = run64.residuals(norms, infos);
-          tracer.step("sweep", fp64_iter, max_res, norms);
-          if (max_res <= cfg.tol) { converged = true; break; }
-          refine.shadow();
-        }
-        refine.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
-        exact = false;
-      }
+    for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
+      max_res = run64.residuals(norms, infos);
+      tracer.step("fp64", fp64_iter, max_res, norms);
+      if (max_res <= cfg.tol) { converged = true; break; }
+      run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
     }
     fp64_iter = std::min(fp64_iter, cfg.max_iter);
     iter += fp64_iter;

@@ -280,24 +280,3 @@ def test_band_chunk_and_tuning_change_no_result(precision, hfo2):
             eig = [ctx.solve((0, 0, 0), w.nbands)[0] for _ in range(4)]
             for e in eig[1:]:
                 assert np.array_equal(e, eig[0])
-
-
-@pytest.mark.parametrize("name", ["si2", "hfo2"])
-def test_mixed_refinement_matches_dense(name, si2, hfo2, oracle_system, monkeypatch):
-    """The mixed refinement (HALF_REFINE=mixed: FP64 X blocks, FP32 corrections
-    on the tensor cores, an exact FP64 sweep before convergence) reaches the
-    dense FP64 eigenvalues to 1e-8 eV, like the FP64 refinement."""
-    from oracle import hamiltonian as H
-    files = {"si2": si2, "hfo2": hfo2}[name]
-    w = files[0]
-    op = H.prepare(oracle_system(name, files))
-    nb = 8 if name == "si2" else w.nbands
-    ref, _, _, _ = H.solve_dense(op, nb)
-    with ctx_for(files) as ctx:
-        for refine in ("fp64", "mixed"):
-            monkeypatch.setenv("HALF_REFINE", refine)
-            ctx.set_acc(tol=2e-5 if name == "hfo2" else 1e-7, max_iterations=400, precision="mixed")
-            e, _, _, _ = ctx.solve((0, 0, 0), nb)
-            info = ctx.info()
-            assert info["converged"] == 1, refine
-            assert np.abs(e - ref).max() <= 1e-8, (refine, np.abs(e - ref).max())
