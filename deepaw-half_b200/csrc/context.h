@@ -75,6 +75,7 @@ struct Runtime {
   bool bf16x9 = false;   // cuBLAS offers FP32 emulation on BF16 tensor cores
   bool tc_gemm = true;   // complex FP32 GEMMs on the library's tcgen05 kernel (tc_gemm.cu)
   DeviceBuffer<unsigned char> tc_work;   // its split-K partial sums, grow-only
+  DeviceBuffer<unsigned char> tc_planes; // its operands pre-split into bf16 planes, grow-only
   DeviceBuffer<int> tc_err;              // raised when one of its pipeline waits gave up
   Profile prof;
   Runtime();

@@ -78,6 +78,21 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   }
 }
 
+// Adds `bytes` to the transaction count the current phase of `bar` waits for
+// (no arrival); the bulk copies below complete them.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.shared::cta.b64 [%1], %0;" ::"r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// Bulk (TMA) copy of `bytes` contiguous bytes from this GPU's global memory to
+// shared memory, completing `bytes` transactions on `bar`.  No multicast.
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 // Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -205,6 +205,50 @@ __device__ __forceinline__ void store_chunk8(const float2 (&v)[8], uint32_t base
   for (int p = 0; p < 4; ++p) st_shared_v4(base + uint32_t(p) * pstride + off, w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
+// Pre-split planes of a dense operand.  Element (r, k) of op(.) (zero outside
+// the matrix, r < rows_pad, k < 16 nkb) goes to the four bf16 planes (Re hi,
+// Re lo, Im hi, Im lo), plane p at out + p plane_bytes, k block kb at
+// kb rows_pad 32 bytes, and inside it the K-major core-matrix layout
+// (r/8) 256 + (k/8) 128 + (r%8) 16 + (k%8) 2: the tile layout in shared
+// memory, so the tile of any 8-aligned row range is ONE contiguous bulk copy.
+// One thread per (row, 8 consecutive k): consecutive threads take consecutive
+// rows, so row-contiguous operands load coalesced and each group of 8 rows
+// stores 128 contiguous bytes per plane.
+__global__ void presplit_kernel(TcOperand op, int rows_pad, int nkb, unsigned char* __restrict__ out,
+                                long long plane_bytes) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)rows_pad * nkb * 2) return;
+  const int r = int(t % rows_pad);
+  const long long o = t / rows_pad;
+  const int kb = int(o >> 1), half = int(o & 1), k0 = int(o * 8);
+  float2 v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int k = k0 + i;
+    float2 x = make_float2(0.f, 0.f);
+    if (r < op.rows && k < op.kdim) {
+      if (op.kind == TcOperand::kDenseK) {
+        const float2* src = r < op.split ? op.p + (long long)r * op.ld : op.p2 + (long long)(r - op.split) * op.ld;
+        x = __ldg(src + k);
+      } else {
+        x = __ldg(op.p + r + (long long)k * op.ld);
+      }
+      if (op.conj) x.y = -x.y;
+    }
+    v[i] = x;
+  }
+  uint32_t w[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    split_pair(v[2 * i].x, v[2 * i + 1].x, w[0][i], w[1][i]);
+    split_pair(v[2 * i].y, v[2 * i + 1].y, w[2][i], w[3][i]);
+  }
+  const long long off = (long long)kb * rows_pad * 32 + (long long)(r >> 3) * 256 + half * 128 + (r & 7) * 16;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    *reinterpret_cast<uint4*>(out + p * plane_bytes + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+}
+
 // Projector element for column `col` at plane wave g (g0..g2 = n + k), conj
 // or not; `atom_c` caches the phase of the last atom seen.
 __device__ __forceinline__ float2 projector_value(const TcOperand& op, int col, int g, double g0, double g1, double g2,
@@ -302,7 +346,8 @@ __device__ __forceinline__ void store_operand(const TcOperand& op, int r0, int R
     case TcOperand::kDenseK: store_dense_k(op, R, base, pstride, warp, lane, v); break;
     case TcOperand::kDenseMN: store_dense_mn(op, R, base, pstride, warp, lane, v); break;
     case TcOperand::kProjConj: fill_proj_conj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
-    default: fill_proj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
+    case TcOperand::kProj: fill_proj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
+    default: break;   // kPlanes: bulk copies fill the stage
   }
 }
 
@@ -338,6 +383,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool a_mn = is_mn(A.kind), b_mn = is_mn(B.kind);
   const uint32_t a_ps = plane_stride(kBM, a_mn), b_ps = plane_stride(bn, b_mn);
   const uint32_t sbytes = stage_bytes(bn, A.kind, B.kind);
+  const uint32_t bulk_bytes = (A.kind == TcOperand::kPlanes ? 4u * kBM * 32u : 0u) +
+                              (B.kind == TcOperand::kPlanes ? 4u * uint32_t(bn) * 32u : 0u);
   uint32_t tcols = 32;
   while (tcols < uint32_t(2 * bn)) tcols <<= 1;
   const uint32_t ci_off = tcols >> 1;
@@ -382,6 +429,20 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
           const int k0 = (kb0 + ii) * kBK;
+          if (bulk_bytes && warp == 0 && lane == 0) {   // pre-split operands: one bulk copy per plane
+            mbar_expect_tx(&full_bar[s], bulk_bytes);
+            const long long kb = kb0 + ii;
+            if (A.kind == TcOperand::kPlanes)
+              for (int p = 0; p < 4; ++p)
+                bulk_copy_g2s(abase + uint32_t(p) * a_ps,
+                              A.planes + p * A.plane_bytes + kb * A.rows_pad * 32 + (long long)m0 * 32,
+                              uint32_t(kBM * 32), &full_bar[s]);
+            if (B.kind == TcOperand::kPlanes)
+              for (int p = 0; p < 4; ++p)
+                bulk_copy_g2s(bbase + uint32_t(p) * b_ps,
+                              B.planes + p * B.plane_bytes + kb * B.rows_pad * 32 + (long long)n0 * 32,
+                              uint32_t(bn * 32), &full_bar[s]);
+          }
           store_operand(A, m0, kBM, k0, abase, a_ps, warp, lane, va[h]);
           store_operand(B, n0, bn, k0, bbase, b_ps, warp, lane, vb[h]);
           fence_proxy_async_smem();
@@ -541,7 +602,49 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     tune_token = Tuner::begin(key, idx, st);
   }
   const int nt = (N + bn - 1) / bn;
-  const size_t smem = size_t(kStages) * stage_bytes(bn, A.kind, B.kind) + kSmemSlack;
+  // Dense operands are split once into bf16 planes in global memory by a
+  // bandwidth-bound pass; the GEMM then feeds its stages by bulk copies.
+  // Generated projector operands keep their in-kernel producers.
+  TcOperand Ak = A, Bk = B;
+  Profile& pf = rt.prof;
+  int span0 = -1;
+  if (nkb > 0) {
+    auto dense = [](const TcOperand& o) { return o.kind == TcOperand::kDenseK || o.kind == TcOperand::kDenseMN; };
+    const int rpa = mt * kBM, rpb = nt * bn;
+    const long long pa = dense(A) ? (long long)rpa * nkb * 32 : 0, pb = dense(B) ? (long long)rpb * nkb * 32 : 0;
+    if (pa + pb > 0) {
+      const size_t bytes = size_t(4) * size_t(pa + pb);
+      if (rt.tc_planes.size() < bytes) rt.tc_planes.resize(bytes);
+      unsigned char* planes = rt.tc_planes.get();
+      span0 = pf.record(st);
+      if (pa > 0) {
+        const long long th = (long long)rpa * nkb * 2;
+        presplit_kernel<<<ceil_div(th, 256), 256, 0, st>>>(A, rpa, nkb, planes, pa);
+        Ak = TcOperand();
+        Ak.kind = TcOperand::kPlanes;
+        Ak.rows = A.rows;
+        Ak.kdim = A.kdim;
+        Ak.planes = planes;
+        Ak.plane_bytes = pa;
+        Ak.rows_pad = rpa;
+        ++pf.launches;
+      }
+      if (pb > 0) {
+        const long long th = (long long)rpb * nkb * 2;
+        presplit_kernel<<<ceil_div(th, 256), 256, 0, st>>>(B, rpb, nkb, planes + 4 * pa, pb);
+        Bk = TcOperand();
+        Bk.kind = TcOperand::kPlanes;
+        Bk.rows = B.rows;
+        Bk.kdim = B.kdim;
+        Bk.planes = planes + 4 * pa;
+        Bk.plane_bytes = pb;
+        Bk.rows_pad = rpb;
+        ++pf.launches;
+      }
+      HALF_LAUNCH("tensor-core operand split");
+    }
+  }
+  const size_t smem = size_t(kStages) * stage_bytes(bn, Ak.kind, Bk.kind) + kSmemSlack;
   raise_smem_limit(tc_cgemm_kernel, smem);
   Out o{};
   o.alpha = alpha;
@@ -562,9 +665,8 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     o.c = rt.tc_work.get();
   }
   if (nkb > 0) {
-    Profile& pf = rt.prof;
-    const int e0 = pf.record(st);
-    tc_cgemm_kernel<<<dim3(mt, nt, splits), kThreads, smem, st>>>(A, B, bn, kbps, nkb, o, rt.tc_err.get());
+    const int e0 = span0 >= 0 ? span0 : pf.record(st);
+    tc_cgemm_kernel<<<dim3(mt, nt, splits), kThreads, smem, st>>>(Ak, Bk, bn, kbps, nkb, o, rt.tc_err.get());
     HALF_LAUNCH("tensor-core cgemm");
     Tuner::finish(tune_token, st, 1.0);
     pf.span(Profile::kTensor, e0, pf.record(st));

@@ -20,7 +20,8 @@ struct TcOperand {
     kDenseK = 0,      // element (r, k) at p[k + r ld]: k contiguous
     kDenseMN = 1,     // element (r, k) at p[r + k ld]: r contiguous
     kProjConj = 2,    // conj(B[g = k, col = r]): rows = projector columns, k = plane waves
-    kProj = 3         // B[g = r, col = k]: rows = plane waves, k = projector columns
+    kProj = 3,        // B[g = r, col = k]: rows = plane waves, k = projector columns
+    kPlanes = 4       // pre-split bf16 planes in global memory (set up by tc_cgemm itself)
   };
   int kind = kDenseK;
   int rows = 0, kdim = 0;
@@ -36,6 +37,11 @@ struct TcOperand {
   const double* afrac = nullptr;   // per atom: (q.R) / (2 pi) = sum_j (n_j + k_j) afrac[3 a + j]
   double kf0 = 0, kf1 = 0, kf2 = 0;
   int npw = 0;
+  // kPlanes: plane p (Re hi, Re lo, Im hi, Im lo) at planes + p plane_bytes;
+  // k block kb at kb rows_pad 32 bytes, in the tile's shared-memory layout
+  const unsigned char* planes = nullptr;
+  long long plane_bytes = 0;
+  int rows_pad = 0;
 };
 
 // op(A) (M x K) and op(B) (K x N) from cuBLAS-style operations on column-major storage.
