@@ -234,7 +234,7 @@ def test_guarded_and_mixed_match_dense_on_the_64_atom_cell(inputs_dir):
 
 @pytest.mark.parametrize("name", ["si2", "hfo2"])
 def test_soft_locking_matches_dense(name, si2, hfo2, oracle_system, monkeypatch):
-    """Soft locking (HALF_SOFT_LOCK=1, guard-band modes): requested bands whose
+    """Soft locking (the guard-band modes' default; HALF_SOFT_LOCK=0 turns it off): requested bands whose
     residual is at or below half the tolerance add no correction direction, so
     the Rayleigh-Ritz pencils shrink; the converged eigenvalues must still be
     the dense solve's, and the operator must see fewer columns than without."""
