@@ -17,8 +17,8 @@
 //                Im += Ar_h Bi_h + Ar_h Bi_l + Ar_l Bi_h + Ai_h Br_h + Ai_h Br_l + Ai_l Br_h
 //              (the minus through the instruction descriptor's negate-A bit)
 //              and commits each stage back to the producers.
-// Four stages of mbarrier-synchronised shared-memory buffers overlap the
-// producers with the tensor core.  Every wait is bounded (tc.cuh): a stuck
+// Up to eight stages of mbarrier-synchronised shared-memory buffers (as many
+// as fit) overlap the loads with the tensor core.  Every wait is bounded (tc.cuh): a stuck
 // pipeline raises the runtime's error flag instead of hanging the GPU.
 //
 // Shared-memory plane layouts (bytes; the producers choose the layout that
@@ -45,7 +45,8 @@ using namespace tc;
 
 constexpr int kBM = 128;
 constexpr int kBK = 16;
-constexpr int kStages = 4;
+constexpr int kMaxPipe = 8;          // stages: as many as fit the shared memory, up to this
+constexpr size_t kSmemBudget = 225 * 1024;   // dynamic shared memory the stages may use
 constexpr int kProdWarps = 8;
 constexpr int kProdThreads = kProdWarps * 32;
 constexpr int kThreads = kProdThreads + 32;
@@ -370,9 +371,9 @@ __device__ __forceinline__ void write_out(T* dst, double re, double im, const Ou
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_cgemm_kernel(TcOperand A, TcOperand B, int bn, int kb_per_split, int nkb_total, Out out, int* err) {
+    tc_cgemm_kernel(TcOperand A, TcOperand B, int bn, int nst, int kb_per_split, int nkb_total, Out out, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
-  __shared__ uint64_t full_bar[kStages], empty_bar[kStages], accum_bar;
+  __shared__ uint64_t full_bar[kMaxPipe], empty_bar[kMaxPipe], accum_bar;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == kProdWarps) tmem_alloc(&tmem_slot, tcols);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < nst; ++s) {
       mbar_init(&full_bar[s], kProdWarps);
       mbar_init(&empty_bar[s], 1);
     }
@@ -422,8 +423,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             load_operand(A, m0, kBM, (kb0 + ii + 1) * kBK, warp, lane, va[h ^ 1]);
             load_operand(B, n0, bn, (kb0 + ii + 1) * kBK, warp, lane, vb[h ^ 1]);
           }
-          const int s = ii % kStages;
-          if (ii >= kStages && !__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ((ii / kStages) - 1) & 1, abort))) {
+          const int s = ii % nst;
+          if (ii >= nst && !__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ((ii / nst) - 1) & 1, abort))) {
             i = nkb;   // leave both loops
             break;
           }
@@ -487,8 +488,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t id_pos = instr_desc_bf16(bn, false, a_mn, b_mn), id_neg = instr_desc_bf16(bn, true, a_mn, b_mn);
     const uint32_t a_sbo = a_mn ? 272u : 256u, b_sbo = b_mn ? 272u : 256u;
     for (int i = 0; i < nkb; ++i) {
-      const int s = i % kStages;
-      if (!mbar_wait(&full_bar[s], (i / kStages) & 1, abort)) break;
+      const int s = i % nst;
+      if (!mbar_wait(&full_bar[s], (i / nst) & 1, abort)) break;
       tcgen05_fence_after();
       const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
 #pragma unroll
@@ -644,7 +645,10 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
       HALF_LAUNCH("tensor-core operand split");
     }
   }
-  const size_t smem = size_t(kStages) * stage_bytes(bn, Ak.kind, Bk.kind) + kSmemSlack;
+  const size_t sbytes = stage_bytes(bn, Ak.kind, Bk.kind);
+  const int nst = int(std::min<size_t>(kMaxPipe, (kSmemBudget - kSmemSlack) / sbytes));
+  if (nst < 2) fail(kInternal, "tensor-core GEMM stage does not fit shared memory twice");
+  const size_t smem = size_t(nst) * sbytes + kSmemSlack;
   raise_smem_limit(tc_cgemm_kernel, smem);
   Out o{};
   o.alpha = alpha;
@@ -666,7 +670,7 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
   }
   if (nkb > 0) {
     const int e0 = span0 >= 0 ? span0 : pf.record(st);
-    tc_cgemm_kernel<<<dim3(mt, nt, splits), kThreads, smem, st>>>(Ak, Bk, bn, kbps, nkb, o, rt.tc_err.get());
+    tc_cgemm_kernel<<<dim3(mt, nt, splits), kThreads, smem, st>>>(Ak, Bk, bn, nst, kbps, nkb, o, rt.tc_err.get());
     HALF_LAUNCH("tensor-core cgemm");
     Tuner::finish(tune_token, st, 1.0);
     pf.span(Profile::kTensor, e0, pf.record(st));
