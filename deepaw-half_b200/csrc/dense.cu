@@ -8,6 +8,7 @@
 // Here the two projector sums are one GEMM each, (B . blockdiag(D)) B^H.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "blas.h"
 #include "context.h"
@@ -140,6 +141,127 @@ void assemble_dense(Context& ctx, KOperatorSet& ks, double2* h, double2* s) {
   HALF_CUDA(cudaStreamSynchronize(st));
 }
 
+namespace {
+
+// Orders above this go through the 64-bit solver API: the workspace queries of
+// zheevd / zhegvd return an int count of complex elements, which overflows near
+// n = 2^15 (measured: the 38,089-plane-wave Gamma point of the 216-atom cell).
+// HALF_DENSE_64BIT_ORDER lowers the switch point (tests exercise the 64-bit
+// path at small orders with it).
+long long dense_64bit_order() {
+  const char* e = std::getenv("HALF_DENSE_64BIT_ORDER");
+  if (e && *e) return std::atoll(e);
+  return 16384;
+}
+
+struct DnParams {
+  cusolverDnParams_t p = nullptr;
+  DnParams() { cusolver_check(cusolverDnCreateParams(&p), "params"); }
+  ~DnParams() { if (p) cusolverDnDestroyParams(p); }
+  DnParams(const DnParams&) = delete;
+  DnParams& operator=(const DnParams&) = delete;
+};
+
+struct Work64 {
+  DeviceBuffer<unsigned char> dev;
+  std::vector<unsigned char> host;
+  void reserve(size_t d, size_t hb) {
+    if (d > dev.size()) dev.resize(d);
+    if (hb > host.size()) host.resize(hb);
+  }
+};
+
+int read_info(const DeviceBuffer<int>& info, cudaStream_t st) {
+  int h = 0;
+  HALF_CUDA(cudaMemcpyAsync(&h, info.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  HALF_CUDA(cudaStreamSynchronize(st));
+  return h;
+}
+
+// Eigenvalues (and, with vectors, eigenvectors in place) of the Hermitian
+// matrix A through the 64-bit API; with index_range only the lowest nbands.
+void heevd64(Runtime& rt, const DnParams& prm, Work64& ws, bool vectors, bool index_range, long long n, int nbands,
+             double2* A, double* w, DeviceBuffer<int>& info) {
+  const cusolverEigMode_t jobz = vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+  size_t dbytes = 0, hbytes = 0;
+  if (index_range) {
+    double vl = 0, vu = 0;
+    int64_t meig = 0;
+    cusolver_check(cusolverDnXsyevdx_bufferSize(rt.solver, prm.p, jobz, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, n,
+                                                CUDA_C_64F, A, n, &vl, &vu, 1, nbands, &meig, CUDA_R_64F, w,
+                                                CUDA_C_64F, &dbytes, &hbytes),
+                   "Xsyevdx buffer");
+    ws.reserve(dbytes, hbytes);
+    cusolver_check(cusolverDnXsyevdx(rt.solver, prm.p, jobz, CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, n,
+                                     CUDA_C_64F, A, n, &vl, &vu, 1, nbands, &meig, CUDA_R_64F, w, CUDA_C_64F,
+                                     ws.dev.get(), ws.dev.size(), ws.host.data(), ws.host.size(), info.get()),
+                   "Xsyevdx");
+    if (read_info(info, rt.stream) != 0 || meig != nbands) fail(kInternal, "VASP-like generalized eigensolve failed");
+    return;
+  }
+  cusolver_check(cusolverDnXsyevd_bufferSize(rt.solver, prm.p, jobz, CUBLAS_FILL_MODE_UPPER, n, CUDA_C_64F, A, n,
+                                             CUDA_R_64F, w, CUDA_C_64F, &dbytes, &hbytes),
+                 "Xsyevd buffer");
+  ws.reserve(dbytes, hbytes);
+  cusolver_check(cusolverDnXsyevd(rt.solver, prm.p, jobz, CUBLAS_FILL_MODE_UPPER, n, CUDA_C_64F, A, n, CUDA_R_64F, w,
+                                  CUDA_C_64F, ws.dev.get(), ws.dev.size(), ws.host.data(), ws.host.size(), info.get()),
+                 "Xsyevd");
+  if (read_info(info, rt.stream) != 0) fail(kInternal, "eigensolve failed");
+}
+
+// The generalized problem H X = S X w at large order, the steps zhegvd takes:
+// S = U^H U (Cholesky, upper), C = U^-H H U^-1 (two triangular solves),
+// C Z = Z w, X = U^-1 Z.  H is overwritten by X, S by U.
+void solve_dense_64(Runtime& rt, long long n, int nbands, bool index_range, bool vectors, double2* h, double2* s,
+                    double* w, SolveOutput& out) {
+  cudaStream_t st = rt.stream;
+  DnParams prm;
+  Work64 ws;
+  DeviceBuffer<int> info(1);
+  if (!index_range) {
+    // overlap extremes from the eigenvalues of S (src/half_cuda_solver.cuf:146-150)
+    DeviceBuffer<double2> s2((size_t)n * n);
+    HALF_CUDA(cudaMemcpyAsync(s2.get(), s, (size_t)n * n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    heevd64(rt, prm, ws, false, false, n, nbands, s2.get(), w, info);
+    double lo = 0, hi = 0;
+    HALF_CUDA(cudaMemcpyAsync(&lo, w, sizeof(double), cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaMemcpyAsync(&hi, w + n - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    HALF_CUDA(cudaStreamSynchronize(st));
+    out.overlap_min = lo;
+    out.overlap_max = hi;
+  } else {
+    out.overlap_min = -1.0;
+    out.overlap_max = -1.0;
+  }
+  size_t dbytes = 0, hbytes = 0;
+  cusolver_check(cusolverDnXpotrf_bufferSize(rt.solver, prm.p, CUBLAS_FILL_MODE_UPPER, n, CUDA_C_64F, s, n, CUDA_C_64F,
+                                             &dbytes, &hbytes),
+                 "Xpotrf buffer");
+  ws.reserve(dbytes, hbytes);
+  cusolver_check(cusolverDnXpotrf(rt.solver, prm.p, CUBLAS_FILL_MODE_UPPER, n, CUDA_C_64F, s, n, CUDA_C_64F,
+                                  ws.dev.get(), ws.dev.size(), ws.host.data(), ws.host.size(), info.get()),
+                 "Xpotrf");
+  if (read_info(info, st) != 0) fail(kInternal, "generalized eigensolve failed (overlap not positive definite)");
+  const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
+  auto* H = reinterpret_cast<cuDoubleComplex*>(h);
+  auto* U = reinterpret_cast<const cuDoubleComplex*>(s);
+  cublas_check(cublasZtrsm_64(rt.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT, n,
+                              n, &one, U, n, H, n),
+               "ztrsm U^-H H");
+  cublas_check(cublasZtrsm_64(rt.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n,
+                              n, &one, U, n, H, n),
+               "ztrsm H U^-1");
+  heevd64(rt, prm, ws, vectors, index_range, n, nbands, h, w, info);
+  if (vectors) {
+    // only the first nbands columns of Z are kept
+    cublas_check(cublasZtrsm_64(rt.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                                n, nbands, &one, U, n, H, n),
+                 "ztrsm U^-1 Z");
+  }
+}
+
+}  // namespace
+
 void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, bool want_vectors, SolveOutput& out) {
   Runtime& rt = *ks.rt;
   cudaStream_t st = rt.stream;
@@ -154,7 +276,9 @@ void solve_dense(Context& ctx, KOperatorSet& ks, int nbands, bool index_range, b
   int lwork = 0, hinfo = 0;
   // eigenvectors are formed for the host copy or for a caller that keeps them on the device (forces)
   const bool compute_vectors = want_vectors || out.keep_device;
-  if (index_range) {
+  if (n > dense_64bit_order()) {
+    solve_dense_64(rt, n, nbands, index_range, compute_vectors, h.get(), s.get(), w.get(), out);
+  } else if (index_range) {
     // src/half_cuda_solver.cuf:119-144: only the lowest nbands, no overlap solve
     int meig = 0;
     cusolverEigMode_t jobz = compute_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;

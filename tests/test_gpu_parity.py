@@ -232,6 +232,30 @@ def test_guarded_and_mixed_match_dense_on_the_64_atom_cell(inputs_dir):
             assert np.abs(e - ref).max() <= tol, (precision, np.abs(e - ref).max())
 
 
+@pytest.mark.parametrize("solver,nb", [("evd", 16), ("vasp", 8)])
+def test_dense_64bit_path_matches_oracle(solver, nb, si2, oracle_system, monkeypatch):
+    """Large orders (above 16,384 plane waves) solve through the 64-bit solver API
+    (Cholesky, two triangular solves, Hermitian evd); HALF_DENSE_64BIT_ORDER=0
+    sends this small cell down that path, which must give the oracle's
+    eigenpairs, overlap extremes and S-normalisation like the 32-bit path."""
+    from oracle import hamiltonian as H
+    op = H.prepare(oracle_system("si2", si2))
+    w, _, smin, smax = H.solve_dense(op, nb)
+    h, s = H.assemble_dense(op)
+    monkeypatch.setenv("HALF_DENSE_64BIT_ORDER", "0")
+    with ctx_for(si2, solver=solver) as ctx:
+        eg, _, gmin, gmax = ctx.solve((0, 0, 0), nb)
+        ev, vec, _, _ = ctx.solve((0, 0, 0), nb, vectors=True)
+    assert np.abs(eg - w).max() <= 1e-10
+    assert np.abs(ev - w).max() <= 1e-10
+    if solver == "evd":
+        assert abs(gmin - smin) <= 1e-10 and abs(gmax - smax) <= 1e-10
+    else:
+        assert gmin == -1.0 and gmax == -1.0
+    assert np.abs(h @ vec - (s @ vec) * ev[None, :]).max() <= 1e-9
+    assert np.abs(vec.conj().T @ s @ vec - np.eye(nb)).max() <= 1e-10
+
+
 @pytest.mark.parametrize("name", ["si2", "hfo2"])
 def test_soft_locking_matches_dense(name, si2, hfo2, oracle_system, monkeypatch):
     """Soft locking (the guard-band modes' default; HALF_SOFT_LOCK=0 turns it off): requested bands whose
