@@ -190,8 +190,8 @@ struct KOperatorSet {
   std::unique_ptr<KOperator<double>> op64;
   std::unique_ptr<KOperator<float>> op32;
   DeviceBuffer<double> qvec;                  // npw*3 (forces)
-  // Tables that generate the projector matrix in-tile (the FP32 operator's
-  // GEMMs and the FP64 force adjoint): B[g, col] = ftab64[frow][g] (-i)^l
+  // Tables that generate the projector matrix (the FP32 operator's bf16
+  // planes and, in-tile, the FP64 force adjoint): B[g, col] = ftab64[frow][g] (-i)^l
   // exp(-2 pi i sum_j (n_j(g) + k_j) afrac[3 atom + j]), pcol[col] =
   // (atom << 16) | (frow << 2) | l, gpack[g] = (n1, n2, n3) as signed 10-bit fields.
   DeviceBuffer<double> ftab64, afrac;

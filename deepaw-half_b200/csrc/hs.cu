@@ -21,10 +21,12 @@
 // projector part is one GEMM B^H X over all species and bands, a D/Q mixing
 // kernel and the GEMMs accumulating B DY into H X and B QY into S X.  In FP64
 // B is stored and the GEMMs are cuBLAS ZGEMM (the reference's calls); in FP32
-// B is never stored: the tensor-core GEMM (tc_gemm.cu) generates its tiles
-// from a per-k radial-angular table (Omega^-1/2 beta_l(|q|) Y_lm, one row per
-// species channel), the packed plane-wave indices and the ions' b_j.R / 2 pi,
-// and B [DY | QY] is one GEMM with a doubled N writing H X and S X.
+// one pass per k point generates B from a radial-angular table
+// (Omega^-1/2 beta_l(|q|) Y_lm, one row per species channel), the packed
+// plane-wave indices and the ions' b_j.R / 2 pi straight into the bf16 planes
+// of the tensor-core GEMM (tc_gemm.cu), in both orientations (conj(B)^T and
+// B; 8 bytes per element each), and B [DY | QY] is one GEMM with a doubled N
+// writing H X and S X.
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -46,13 +48,17 @@ struct KOperator {
   DeviceBuffer<C> work;      // chunk x nplanes x n2 x n3
   int work_chunk = 0;
   DeviceBuffer<C> B;         // FP64: npw x np, column-major
-  // FP32: the projector matrix is generated inside the tensor-core GEMM tiles
-  // (tc_gemm.cu) from these tables instead of being stored
+  // FP32: the projector matrix is generated from these tables straight into
+  // the bf16 planes of the tensor-core GEMM (tc_gemm.cu), once per k point,
+  // in the two orientations the products use
   DeviceBuffer<float> ftab;  // [frow][npw] Omega^-1/2 beta_l(|q|) Y_lm(q^), frow = (species, channel, m)
   DeviceBuffer<int> gpack;   // npw packed (n1, n2, n3)
   DeviceBuffer<int> pcol;    // np: (ion << 16) | (frow << 2) | l
   DeviceBuffer<double> afrac;   // nions x 3: b_j . R / 2 pi
   double kf[3] = {0, 0, 0};
+  DeviceBuffer<unsigned char> bh_store, b_store;
+  TcOperand bh_planes;       // conj(B)^T: np x npw
+  TcOperand b_planes;        // B: npw x np
   DeviceBuffer<R> dall, qall;            // D per atom, Q per species
   DeviceBuffer<int> col_base, col_a, col_nlm, col_dofs, col_qofs;
   DeviceBuffer<C> coeff, dy, qy;
@@ -401,6 +407,23 @@ void fill_operator(Context& ctx, Runtime& rt, const Basis& basis, const HostGeom
     op.pcol.upload(gen.pcol, s);
     op.afrac.upload(gen.afrac, s);
     for (int j = 0; j < 3; ++j) op.kf[j] = basis.kpoint[j];
+    TcOperand g;
+    g.kind = TcOperand::kProjConj;
+    g.rows = np;
+    g.kdim = op.npw;
+    g.ftab = op.ftab.get();
+    g.gpack = op.gpack.get();
+    g.pcol = op.pcol.get();
+    g.afrac = op.afrac.get();
+    g.kf0 = op.kf[0];
+    g.kf1 = op.kf[1];
+    g.kf2 = op.kf[2];
+    g.npw = op.npw;
+    op.bh_planes = tc_presplit_a(rt, g, op.bh_store);
+    g.kind = TcOperand::kProj;
+    g.rows = op.npw;
+    g.kdim = np;
+    op.b_planes = tc_presplit_a(rt, g, op.b_store);
   }
   std::vector<double> dall, qall;
   for (auto& sp : ctx.species) {
@@ -512,7 +535,7 @@ std::unique_ptr<KOperatorSet> prepare_operator(Context& ctx, Runtime& rt, const 
   gen.rm2 = drm2.get();
   gen.pref = 1.0 / std::sqrt(ctx.crystal.volume());
   DeviceBuffer<ProjCol> drows;
-  if (np > 0) {   // in-tile generation tables, shared by the FP32 operator and the force adjoint
+  if (np > 0) {   // projector generation tables, shared by the FP32 operator's planes and the force adjoint
     const int nf = int(gen.frows.size());
     drows.upload(gen.frows, s);
     ks->ftab64.resize(size_t(nf) * npw);
@@ -645,32 +668,16 @@ void apply_nonlocal(Runtime& rt, KOperator<R>& op, const cplx_t<R>* x, long long
     ++rt.prof.launches;
   };
   if constexpr (sizeof(R) == 4) {
-    // FP32: B is generated inside the tensor-core tiles (tc_gemm.cu).
+    // FP32: B in bf16 planes split once per k point (fill_operator).
     //   coeff = conj(B)^T X            (np x nb, K = npw)
     //   [H X | S X] += B [DY | QY]     (npw x 2nb, K = np; one GEMM, two outputs)
-    TcOperand bh;
-    bh.kind = TcOperand::kProjConj;
-    bh.rows = op.np;
-    bh.kdim = op.npw;
-    bh.ftab = op.ftab.get();
-    bh.gpack = op.gpack.get();
-    bh.pcol = op.pcol.get();
-    bh.afrac = op.afrac.get();
-    bh.kf0 = op.kf[0];
-    bh.kf1 = op.kf[1];
-    bh.kf2 = op.kf[2];
-    bh.npw = op.npw;
-    tc_cgemm(rt, bh, tc_dense_b(CUBLAS_OP_N, x, ld, op.npw, nb), op.np, nb, op.npw, make_double2(1, 0),
+    tc_cgemm(rt, op.bh_planes, tc_dense_b(CUBLAS_OP_N, x, ld, op.npw, nb), op.np, nb, op.npw, make_double2(1, 0),
              make_double2(0, 0), op.coeff.get(), false, op.np);
     mix();
-    TcOperand b = bh;
-    b.kind = TcOperand::kProj;
-    b.rows = op.npw;
-    b.kdim = op.np;
     TcOperand y = tc_dense_b(CUBLAS_OP_N, op.dy.get(), op.np, op.np, 2 * nb);
     y.p2 = op.qy.get();
     y.split = nb;
-    tc_cgemm(rt, b, y, op.npw, 2 * nb, op.np, make_double2(1, 0), make_double2(1, 0), hx, false, ld, sx, nb);
+    tc_cgemm(rt, op.b_planes, y, op.npw, 2 * nb, op.np, make_double2(1, 0), make_double2(1, 0), hx, false, ld, sx, nb);
   } else {
     gemm(rt, CUBLAS_OP_C, CUBLAS_OP_N, op.np, nb, op.npw, one, op.B.get(), op.npw, x, ld, zero, op.coeff.get(), op.np);
     mix();

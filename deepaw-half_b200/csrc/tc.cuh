@@ -1,6 +1,6 @@
 // sm_100a primitives for the tensor-core GEMM (tc_gemm.cu): mbarriers with
-// bounded waits, the async-proxy fence, Tensor Memory allocation, tcgen05.mma
-// with shared-memory descriptors, tcgen05.commit and tcgen05.ld.
+// bounded waits, bulk global->shared copies, Tensor Memory allocation,
+// tcgen05.mma with shared-memory descriptors, tcgen05.commit and tcgen05.ld.
 //
 // Descriptor encodings follow the sm_100 UMMA definitions:
 //   shared-memory descriptor (64 bit): start address >> 4 in [0,14),
@@ -78,6 +78,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   }
 }
 
+// Waits for the phase of `parity` to complete whatever `abort` says, for at
+// most kWaitLimitNs: used to let copies and MMAs in flight land before a CTA
+// that gave up leaves.
+__device__ __forceinline__ bool mbar_wait_drain(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (global_ns() - t0 <= kWaitLimitNs)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
 // Adds `bytes` to the transaction count the current phase of `bar` waits for
 // (no arrival); the bulk copies below complete them.
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
@@ -91,11 +102,6 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uin
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(smem_addr(bar))
                : "memory");
-}
-
-// Generic-proxy shared-memory writes -> visible to the tensor core (async proxy).
-__device__ __forceinline__ void fence_proxy_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ void tcgen05_fence_before() {
@@ -160,13 +166,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v) {
-  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
-}
 
 }  // namespace tc
 }  // namespace hb

@@ -1,32 +1,33 @@
-// Complex FP32 GEMM on the sm_100a tensor cores (tcgen05), with the mixed
-// mode's operands split into bf16 hi/lo planes inside the kernel.
+// Complex FP32 GEMM on the sm_100a tensor cores (tcgen05) for the mixed
+// mode, on operands split into bf16 hi/lo planes.
 //
-// One CTA computes a 128 x BN tile of C (BN <= 256, a multiple of 16) over a
-// range of k blocks (split-K when the tile grid alone cannot fill the GPU).
-//   warps 0-7  producers: read a 128 x 16 slice of op(A) and a BN x 16 slice
-//              of op(B) per stage (dense complex FP32 from global memory, or
-//              projector elements generated from their tables), split every
-//              real and imaginary part into x_hi = bf16(x), x_lo =
-//              bf16(x - x_hi) and store the four planes (Re hi, Re lo,
-//              Im hi, Im lo) of each operand in the canonical no-swizzle
-//              UMMA layout; then, after the last stage, the epilogue
-//              (tcgen05.ld of the accumulators, alpha / beta, stores);
-//   warp 8     one thread issues, per stage, the 12 tcgen05.mma of the
-//              three-term split complex product into two TMEM accumulators
+// Every operand is first split, by a bandwidth-bound pass (presplit_kernel),
+// or once per k point for the projector matrix, into four bf16 planes
+// (Re hi, Re lo, Im hi, Im lo; x_hi = bf16(x), x_lo = bf16(x - x_hi)) stored
+// in global memory in the tile layout of the tensor core, so that the tile of
+// one stage is one contiguous bulk copy per plane.  One CTA then computes a
+// 128 x BN tile of C (BN <= 256, a multiple of 16) over a range of k blocks
+// (split-K when the tile grid alone cannot fill the GPU):
+//   warp 8     one thread: per stage, waits for the stage to be free and
+//              issues the eight bulk copies (cp.async.bulk, no multicast)
+//              that fill it, completing on the stage's full mbarrier;
+//   warp 9     one thread: per stage, the 12 tcgen05.mma of the three-term
+//              split complex product into two TMEM accumulators
 //                Re += Ar_h Br_h + Ar_h Br_l + Ar_l Br_h - (Ai_h Bi_h + Ai_h Bi_l + Ai_l Bi_h)
 //                Im += Ar_h Bi_h + Ar_h Bi_l + Ar_l Bi_h + Ai_h Br_h + Ai_h Br_l + Ai_l Br_h
-//              (the minus through the instruction descriptor's negate-A bit)
-//              and commits each stage back to the producers.
-// Up to eight stages of mbarrier-synchronised shared-memory buffers (as many
-// as fit) overlap the loads with the tensor core.  Every wait is bounded (tc.cuh): a stuck
-// pipeline raises the runtime's error flag instead of hanging the GPU.
+//              (the minus through the instruction descriptor's negate-A bit),
+//              committing each stage back to the producer;
+//   warps 0-7  the epilogue: tcgen05.ld of the accumulators, alpha / beta,
+//              stores (or split-K partial sums).
+// As many stages as fit the shared memory (up to eight) keep the copies
+// ahead of the tensor core.  Every wait is bounded (tc.cuh): a stuck
+// pipeline raises the runtime's error flag instead of hanging the GPU, and
+// the CTA lets its copies and MMAs in flight land before it leaves.
 //
-// Shared-memory plane layouts (bytes; the producers choose the layout that
-// lets a warp's stores hit 32 distinct banks):
-//   K-major  (r, k): (r/8) 256 + (k/8) 128 + (r%8) 16 + (k%8) 2   LBO 128, SBO 256
-//   MN-major (r, k): (r/8) 272 + (k/8) 128 + (k%8) 16 + (r%8) 2   LBO 128, SBO 272
-// Consecutive planes are staggered by 64 bytes so that one store instruction
-// writing a hi plane (even lanes) and a lo plane (odd lanes) is conflict-free.
+// Plane layout (bytes), K-major canonical no-swizzle UMMA layout:
+//   (r, k) of a 16-wide k block: (r/8) 256 + (k/8) 128 + (r%8) 16 + (k%8) 2,
+//   LBO 128, SBO 256; in global memory k block kb of a plane starts at
+//   kb rows_pad 32, so rows r0 .. r0 + R - 1 of it are R 32 contiguous bytes.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -47,20 +48,13 @@ constexpr int kBM = 128;
 constexpr int kBK = 16;
 constexpr int kMaxPipe = 8;          // stages: as many as fit the shared memory, up to this
 constexpr size_t kSmemBudget = 225 * 1024;   // dynamic shared memory the stages may use
-constexpr int kProdWarps = 8;
-constexpr int kProdThreads = kProdWarps * 32;
-constexpr int kThreads = kProdThreads + 32;
-constexpr int kSmemSlack = 128;
+constexpr int kEpiWarps = 8;
+constexpr int kProducerWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
+constexpr int kThreads = (kEpiWarps + 2) * 32;
+constexpr int kSmemSlack = 1024;
 
-__host__ __device__ inline bool is_mn(int kind) {
-  return kind == TcOperand::kDenseMN || kind == TcOperand::kProjConj;
-}
-__host__ __device__ inline uint32_t plane_stride(int rows, bool mn) {
-  const uint32_t bytes = uint32_t(rows / 8) * (mn ? 272u : 256u);
-  return ((bytes + 127u) / 128u) * 128u + 64u;
-}
-__host__ __device__ inline uint32_t stage_bytes(int bn, int akind, int bkind) {
-  const uint32_t s = 4u * plane_stride(kBM, is_mn(akind)) + 4u * plane_stride(bn, is_mn(bkind));
+__host__ __device__ inline uint32_t stage_bytes(int bn) {
+  const uint32_t s = 4u * uint32_t(kBM) * 32u + 4u * uint32_t(bn) * 32u;
   return ((s + 1023u) / 1024u) * 1024u;
 }
 
@@ -84,101 +78,6 @@ __device__ __forceinline__ void split_pair(float a, float b, uint32_t& hi, uint3
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
-// Splits this lane's element and stores, with its neighbour (lane ^ 1), one
-// 4-byte pair per plane: even lanes the hi planes, odd lanes the lo planes.
-// The pair's first element is the even lane's.  Every lane must call this.
-__device__ __forceinline__ void store_pair(float2 v, int lane, uint32_t base, uint32_t pstride, uint32_t off,
-                                           bool store) {
-  uint32_t hi, lo;   // (Re, Im) hi parts and lo parts
-  split_pair(v.x, v.y, hi, lo);
-  const bool even = (lane & 1) == 0;
-  const uint32_t recv = __shfl_xor_sync(0xffffffffu, even ? lo : hi, 1);
-  const uint32_t own = even ? hi : lo;
-  const uint32_t a = even ? own : recv, b = even ? recv : own;
-  if (store) {
-    const uint32_t pr = even ? 0u : 1u;
-    st_shared_u32(base + pr * pstride + off, __byte_perm(a, b, 0x5410));
-    st_shared_u32(base + (pr + 2u) * pstride + off, __byte_perm(a, b, 0x7632));
-  }
-}
-
-// Dense operands are filled in two halves so the producer loop can issue
-// the global loads of stage i + 1 before it splits and stores stage i:
-// load_dense_* brings this warp's elements of one slice into registers (zero
-// outside the matrix), store_dense_* splits and stores them.  NV is the
-// register count per lane: 8 for the 128-row A slice, 16 for B (up to 256 rows).
-
-// k contiguous: each warp step covers 4 rows x 8 k.
-template <int NV>
-__device__ __forceinline__ void load_dense_k(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
-                                             float2 (&v)[NV]) {
-  const int nsteps = (R >> 2) * 2;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int t = warp + i * kProdWarps;
-    v[i] = make_float2(0.f, 0.f);
-    if (t < nsteps) {
-      const int r = r0 + (t >> 1) * 4 + (lane >> 3), k = k0 + (t & 1) * 8 + (lane & 7);
-      if (r < op.rows && k < op.kdim) {
-        const float2* src = r < op.split ? op.p + (long long)r * op.ld : op.p2 + (long long)(r - op.split) * op.ld;
-        v[i] = __ldg(src + k);
-      }
-    }
-  }
-}
-
-template <int NV>
-__device__ __forceinline__ void store_dense_k(const TcOperand& op, int R, uint32_t base, uint32_t pstride, int warp,
-                                              int lane, const float2 (&v)[NV]) {
-  const int nsteps = (R >> 2) * 2;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int t = warp + i * kProdWarps;
-    if (t < nsteps) {
-      const int r = (t >> 1) * 4 + (lane >> 3), kl = (t & 1) * 8 + (lane & 7);
-      float2 x = v[i];
-      if (op.conj) x.y = -x.y;
-      const uint32_t off = uint32_t(r >> 3) * 256u + uint32_t(t & 1) * 128u + uint32_t(r & 7) * 16u +
-                           uint32_t((kl & 7) >> 1) * 4u;
-      store_pair(x, lane, base, pstride, off, true);
-    }
-  }
-}
-
-// rows contiguous: each warp step covers 32 rows at one k.
-template <int NV>
-__device__ __forceinline__ void load_dense_mn(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
-                                              float2 (&v)[NV]) {
-  const int nsteps = ((R + 31) >> 5) * 16;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int t = warp + i * kProdWarps;
-    v[i] = make_float2(0.f, 0.f);
-    if (t < nsteps) {
-      const int rl = (t >> 4) * 32 + lane, r = r0 + rl, k = k0 + (t & 15);
-      if (rl < R && r < op.rows && k < op.kdim) v[i] = __ldg(op.p + r + (long long)k * op.ld);
-    }
-  }
-}
-
-template <int NV>
-__device__ __forceinline__ void store_dense_mn(const TcOperand& op, int R, uint32_t base, uint32_t pstride, int warp,
-                                               int lane, const float2 (&v)[NV]) {
-  const int nsteps = ((R + 31) >> 5) * 16;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    const int t = warp + i * kProdWarps;
-    if (t < nsteps) {
-      const int rl = (t >> 4) * 32 + lane, kl = t & 15, rp = rl & ~1;
-      float2 x = v[i];
-      if (op.conj) x.y = -x.y;
-      const uint32_t off = uint32_t(rp >> 3) * 272u + uint32_t(kl >> 3) * 128u + uint32_t(kl & 7) * 16u +
-                           uint32_t((rp & 7) >> 1) * 4u;
-      store_pair(x, lane, base, pstride, off, rl < R);
-    }
-  }
-}
-
 __device__ __forceinline__ void unpack_g(int gp, double kf0, double kf1, double kf2, double& g0, double& g1,
                                          double& g2) {
   g0 = double((gp << 22) >> 22) + kf0;
@@ -192,62 +91,6 @@ __device__ __forceinline__ void atom_phase(const double* __restrict__ afrac, int
   const double t = g0 * __ldg(afrac + 3 * atom) + g1 * __ldg(afrac + 3 * atom + 1) + g2 * __ldg(afrac + 3 * atom + 2);
   const float fr = float(t - rint(t));
   sincospif(2.0f * fr, &s, &c);
-}
-
-// Eight generated elements -> four 16-byte plane chunks at `off`.
-__device__ __forceinline__ void store_chunk8(const float2 (&v)[8], uint32_t base, uint32_t pstride, uint32_t off) {
-  uint32_t w[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    split_pair(v[2 * i].x, v[2 * i + 1].x, w[0][i], w[1][i]);
-    split_pair(v[2 * i].y, v[2 * i + 1].y, w[2][i], w[3][i]);
-  }
-#pragma unroll
-  for (int p = 0; p < 4; ++p) st_shared_v4(base + uint32_t(p) * pstride + off, w[p][0], w[p][1], w[p][2], w[p][3]);
-}
-
-// Pre-split planes of a dense operand.  Element (r, k) of op(.) (zero outside
-// the matrix, r < rows_pad, k < 16 nkb) goes to the four bf16 planes (Re hi,
-// Re lo, Im hi, Im lo), plane p at out + p plane_bytes, k block kb at
-// kb rows_pad 32 bytes, and inside it the K-major core-matrix layout
-// (r/8) 256 + (k/8) 128 + (r%8) 16 + (k%8) 2: the tile layout in shared
-// memory, so the tile of any 8-aligned row range is ONE contiguous bulk copy.
-// One thread per (row, 8 consecutive k): consecutive threads take consecutive
-// rows, so row-contiguous operands load coalesced and each group of 8 rows
-// stores 128 contiguous bytes per plane.
-__global__ void presplit_kernel(TcOperand op, int rows_pad, int nkb, unsigned char* __restrict__ out,
-                                long long plane_bytes) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= (long long)rows_pad * nkb * 2) return;
-  const int r = int(t % rows_pad);
-  const long long o = t / rows_pad;
-  const int kb = int(o >> 1), half = int(o & 1), k0 = int(o * 8);
-  float2 v[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int k = k0 + i;
-    float2 x = make_float2(0.f, 0.f);
-    if (r < op.rows && k < op.kdim) {
-      if (op.kind == TcOperand::kDenseK) {
-        const float2* src = r < op.split ? op.p + (long long)r * op.ld : op.p2 + (long long)(r - op.split) * op.ld;
-        x = __ldg(src + k);
-      } else {
-        x = __ldg(op.p + r + (long long)k * op.ld);
-      }
-      if (op.conj) x.y = -x.y;
-    }
-    v[i] = x;
-  }
-  uint32_t w[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    split_pair(v[2 * i].x, v[2 * i + 1].x, w[0][i], w[1][i]);
-    split_pair(v[2 * i].y, v[2 * i + 1].y, w[2][i], w[3][i]);
-  }
-  const long long off = (long long)kb * rows_pad * 32 + (long long)(r >> 3) * 256 + half * 128 + (r & 7) * 16;
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-    *reinterpret_cast<uint4*>(out + p * plane_bytes + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
 // Projector element for column `col` at plane wave g (g0..g2 = n + k), conj
@@ -281,75 +124,73 @@ __device__ __forceinline__ float2 projector_value(const TcOperand& op, int col, 
   return make_float2(f * re, f * im);
 }
 
-// conj(B)^T slice: rows = projector columns (MN-major chunks of 8), k = plane waves.
-__device__ __forceinline__ void fill_proj_conj(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                               uint32_t pstride, int tid) {
-  const int tasks = (R >> 3) * 16;
-  for (int t = tid; t < tasks; t += kProdThreads) {
-    const int pc = t >> 4, kl = t & 15, g = k0 + kl;
-    float2 v[8];
-    if (g < op.npw) {
+// Pre-split planes of an operand.  Element (r, k) of op(.) (zero outside the
+// matrix, r < rows_pad, k < 16 nkb) goes to the four bf16 planes, plane p at
+// out + p plane_bytes, in the layout described at the top of this file.
+// One thread per (row, 8 consecutive k): consecutive threads take consecutive
+// rows, so row-contiguous operands load coalesced and each group of 8 rows
+// stores 128 contiguous bytes per plane.  Projector operands generate their
+// elements from the tables (kProj: row = plane wave, k = projector column;
+// kProjConj: row = projector column, k = plane wave).
+__global__ void presplit_kernel(TcOperand op, int rows_pad, int nkb, unsigned char* __restrict__ out,
+                                long long plane_bytes) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)rows_pad * nkb * 2) return;
+  const int r = int(t % rows_pad);
+  const long long o = t / rows_pad;
+  const int kb = int(o >> 1), half = int(o & 1), k0 = int(o * 8);
+  float2 v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = make_float2(0.f, 0.f);
+  if (r < op.rows) {
+    if (op.kind == TcOperand::kProj) {
       double g0, g1, g2;
-      unpack_g(__ldg(op.gpack + g), op.kf0, op.kf1, op.kf2, g0, g1, g2);
+      unpack_g(__ldg(op.gpack + r), op.kf0, op.kf1, op.kf2, g0, g1, g2);
       int atom_c = -1;
       float c = 0.f, s = 0.f;
 #pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (k0 + i < op.kdim) v[i] = projector_value(op, k0 + i, r, g0, g1, g2, false, atom_c, c, s);
+    } else if (op.kind == TcOperand::kProjConj) {
+#pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const int col = r0 + pc * 8 + i;
-        v[i] = col < op.rows ? projector_value(op, col, g, g0, g1, g2, true, atom_c, c, s) : make_float2(0.f, 0.f);
+        const int g = k0 + i;
+        if (g < op.kdim) {
+          double g0, g1, g2;
+          unpack_g(__ldg(op.gpack + g), op.kf0, op.kf1, op.kf2, g0, g1, g2);
+          int atom_c = -1;
+          float c = 0.f, s = 0.f;
+          v[i] = projector_value(op, r, g, g0, g1, g2, true, atom_c, c, s);
+        }
       }
     } else {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = make_float2(0.f, 0.f);
-    }
-    store_chunk8(v, base, pstride, uint32_t(pc) * 272u + uint32_t(kl >> 3) * 128u + uint32_t(kl & 7) * 16u);
-  }
-}
-
-// B slice: rows = plane waves, k = projector columns (K-major chunks of 8).
-__device__ __forceinline__ void fill_proj(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                          uint32_t pstride, int tid) {
-  const int tasks = R * 2;
-  for (int t = tid; t < tasks; t += kProdThreads) {
-    const int row = t % R, kc = t / R, g = r0 + row;
-    float2 v[8];
-    if (g < op.rows) {
-      double g0, g1, g2;
-      unpack_g(__ldg(op.gpack + g), op.kf0, op.kf1, op.kf2, g0, g1, g2);
-      int atom_c = -1;
-      float c = 0.f, s = 0.f;
-#pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const int col = k0 + kc * 8 + i;
-        v[i] = col < op.kdim ? projector_value(op, col, g, g0, g1, g2, false, atom_c, c, s) : make_float2(0.f, 0.f);
+        const int k = k0 + i;
+        if (k < op.kdim) {
+          float2 x;
+          if (op.kind == TcOperand::kDenseK) {
+            const float2* src = r < op.split ? op.p + (long long)r * op.ld : op.p2 + (long long)(r - op.split) * op.ld;
+            x = __ldg(src + k);
+          } else {
+            x = __ldg(op.p + r + (long long)k * op.ld);
+          }
+          if (op.conj) x.y = -x.y;
+          v[i] = x;
+        }
       }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) v[i] = make_float2(0.f, 0.f);
     }
-    store_chunk8(v, base, pstride, uint32_t(row >> 3) * 256u + uint32_t(kc) * 128u + uint32_t(row & 7) * 16u);
   }
-}
-
-template <int NV>
-__device__ __forceinline__ void load_operand(const TcOperand& op, int r0, int R, int k0, int warp, int lane,
-                                             float2 (&v)[NV]) {
-  if (op.kind == TcOperand::kDenseK) load_dense_k(op, r0, R, k0, warp, lane, v);
-  else if (op.kind == TcOperand::kDenseMN) load_dense_mn(op, r0, R, k0, warp, lane, v);
-}
-
-// Generated operands compute their elements here; dense ones store the
-// registers their load_operand brought in.
-template <int NV>
-__device__ __forceinline__ void store_operand(const TcOperand& op, int r0, int R, int k0, uint32_t base,
-                                              uint32_t pstride, int warp, int lane, const float2 (&v)[NV]) {
-  switch (op.kind) {
-    case TcOperand::kDenseK: store_dense_k(op, R, base, pstride, warp, lane, v); break;
-    case TcOperand::kDenseMN: store_dense_mn(op, R, base, pstride, warp, lane, v); break;
-    case TcOperand::kProjConj: fill_proj_conj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
-    case TcOperand::kProj: fill_proj(op, r0, R, k0, base, pstride, warp * 32 + lane); break;
-    default: break;   // kPlanes: bulk copies fill the stage
+  uint32_t w[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    split_pair(v[2 * i].x, v[2 * i + 1].x, w[0][i], w[1][i]);
+    split_pair(v[2 * i].y, v[2 * i + 1].y, w[2][i], w[3][i]);
   }
+  const long long off = (long long)kb * rows_pad * 32 + (long long)(r >> 3) * 256 + half * 128 + (r & 7) * 16;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+    *reinterpret_cast<uint4*>(out + p * plane_bytes + off) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
 }
 
 // (A plane, B plane, accumulator 0 = Re / 1 = Im, negate A)
@@ -370,6 +211,8 @@ __device__ __forceinline__ void write_out(T* dst, double re, double im, const Ou
   *dst = v;
 }
 
+// A and B are pre-split planes (TcOperand::kPlanes); A.rows_pad >= gridDim.x
+// 128 and B.rows_pad >= gridDim.y bn, both with nkb_total k blocks.
 __global__ void __launch_bounds__(kThreads, 1)
     tc_cgemm_kernel(TcOperand A, TcOperand B, int bn, int nst, int kb_per_split, int nkb_total, Out out, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_dyn[];
@@ -381,20 +224,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int kb0 = split * kb_per_split;
   const int nkb = min(nkb_total, kb0 + kb_per_split) - kb0;
   const uint32_t sbase = (smem_addr(smem_dyn) + uint32_t(kSmemSlack - 1)) & ~uint32_t(kSmemSlack - 1);
-  const bool a_mn = is_mn(A.kind), b_mn = is_mn(B.kind);
-  const uint32_t a_ps = plane_stride(kBM, a_mn), b_ps = plane_stride(bn, b_mn);
-  const uint32_t sbytes = stage_bytes(bn, A.kind, B.kind);
-  const uint32_t bulk_bytes = (A.kind == TcOperand::kPlanes ? 4u * kBM * 32u : 0u) +
-                              (B.kind == TcOperand::kPlanes ? 4u * uint32_t(bn) * 32u : 0u);
+  const uint32_t a_ps = uint32_t(kBM) * 32u, b_ps = uint32_t(bn) * 32u;
+  const uint32_t sbytes = stage_bytes(bn);
   uint32_t tcols = 32;
   while (tcols < uint32_t(2 * bn)) tcols <<= 1;
   const uint32_t ci_off = tcols >> 1;
   volatile int* abort = &abort_flag;
 
-  if (warp == kProdWarps) tmem_alloc(&tmem_slot, tcols);
+  if (warp == kMmaWarp) tmem_alloc(&tmem_slot, tcols);
   if (threadIdx.x == 0) {
     for (int s = 0; s < nst; ++s) {
-      mbar_init(&full_bar[s], kProdWarps);
+      mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
     mbar_init(&accum_bar, 1);
@@ -406,54 +246,52 @@ __global__ void __launch_bounds__(kThreads, 1)
   tcgen05_fence_after();
   const uint32_t tmem = tmem_slot;
 
-  if (warp < kProdWarps) {
-    // software pipeline: the dense loads of stage i + 1 are in flight while
-    // stage i is split and stored
-    float2 va[2][8], vb[2][16];
-    if (nkb > 0) {
-      load_operand(A, m0, kBM, kb0 * kBK, warp, lane, va[0]);
-      load_operand(B, n0, bn, kb0 * kBK, warp, lane, vb[0]);
-    }
-    for (int i = 0; i < nkb; i += 2) {
+  if (warp == kProducerWarp) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % nst;
+        if (i >= nst && !mbar_wait(&empty_bar[s], ((i / nst) - 1) & 1, abort)) break;
+        const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
+        const long long kb = kb0 + i;
+        mbar_expect_tx(&full_bar[s], 4u * (a_ps + b_ps));
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int ii = i + h;
-        if (ii < nkb) {
-          if (ii + 1 < nkb) {
-            load_operand(A, m0, kBM, (kb0 + ii + 1) * kBK, warp, lane, va[h ^ 1]);
-            load_operand(B, n0, bn, (kb0 + ii + 1) * kBK, warp, lane, vb[h ^ 1]);
-          }
-          const int s = ii % nst;
-          if (ii >= nst && !__all_sync(0xffffffffu, mbar_wait(&empty_bar[s], ((ii / nst) - 1) & 1, abort))) {
-            i = nkb;   // leave both loops
-            break;
-          }
-          const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
-          const int k0 = (kb0 + ii) * kBK;
-          if (bulk_bytes && warp == 0 && lane == 0) {   // pre-split operands: one bulk copy per plane
-            mbar_expect_tx(&full_bar[s], bulk_bytes);
-            const long long kb = kb0 + ii;
-            if (A.kind == TcOperand::kPlanes)
-              for (int p = 0; p < 4; ++p)
-                bulk_copy_g2s(abase + uint32_t(p) * a_ps,
-                              A.planes + p * A.plane_bytes + kb * A.rows_pad * 32 + (long long)m0 * 32,
-                              uint32_t(kBM * 32), &full_bar[s]);
-            if (B.kind == TcOperand::kPlanes)
-              for (int p = 0; p < 4; ++p)
-                bulk_copy_g2s(bbase + uint32_t(p) * b_ps,
-                              B.planes + p * B.plane_bytes + kb * B.rows_pad * 32 + (long long)n0 * 32,
-                              uint32_t(bn * 32), &full_bar[s]);
-          }
-          store_operand(A, m0, kBM, k0, abase, a_ps, warp, lane, va[h]);
-          store_operand(B, n0, bn, k0, bbase, b_ps, warp, lane, vb[h]);
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&full_bar[s]);
+        for (int p = 0; p < 4; ++p) {
+          bulk_copy_g2s(abase + uint32_t(p) * a_ps, A.planes + p * A.plane_bytes + (kb * A.rows_pad + m0) * 32, a_ps,
+                        &full_bar[s]);
+          bulk_copy_g2s(bbase + uint32_t(p) * b_ps, B.planes + p * B.plane_bytes + (kb * B.rows_pad + n0) * 32, b_ps,
+                        &full_bar[s]);
         }
+        mbar_arrive(&full_bar[s]);
+        issued = i + 1;
+      }
+      if (*abort) {   // let the copies still in flight land before the CTA leaves
+        for (int i = max(0, issued - nst); i < issued; ++i) mbar_wait_drain(&full_bar[i % nst], (i / nst) & 1);
       }
     }
+  } else if (warp == kMmaWarp) {
+    if (lane == 0) {
+      const uint32_t id_pos = instr_desc_bf16(bn, false, false, false), id_neg = instr_desc_bf16(bn, true, false, false);
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % nst;
+        if (!mbar_wait(&full_bar[s], (i / nst) & 1, abort)) break;
+        tcgen05_fence_after();
+        const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+          const uint64_t ad = smem_desc(abase + uint32_t(kCombo[c][0]) * a_ps, 128u, 256u);
+          const uint64_t bd = smem_desc(bbase + uint32_t(kCombo[c][1]) * b_ps, 128u, 256u);
+          mma_bf16(tmem + (kCombo[c][2] ? ci_off : 0u), ad, bd, kCombo[c][3] ? id_neg : id_pos,
+                   i > 0 || (c != 0 && c != 6));
+        }
+        mma_commit(&empty_bar[s]);
+      }
+      mma_commit(&accum_bar);   // also on abort: arrives once every issued MMA has completed
+    }
+  } else {
     // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, every other 16-column chunk
-    if (__all_sync(0xffffffffu, mbar_wait(&accum_bar, 0, abort))) {
+    const bool done = __all_sync(0xffffffffu, mbar_wait_drain(&accum_bar, 0));
+    if (done && !*abort) {
       tcgen05_fence_after();
       const int q = warp & 3, half = warp >> 2;
       const int row = m0 + q * 32 + lane;
@@ -483,29 +321,13 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
+    } else if (!done) {
+      *abort = 1;
     }
-  } else if (lane == 0) {
-    const uint32_t id_pos = instr_desc_bf16(bn, false, a_mn, b_mn), id_neg = instr_desc_bf16(bn, true, a_mn, b_mn);
-    const uint32_t a_sbo = a_mn ? 272u : 256u, b_sbo = b_mn ? 272u : 256u;
-    for (int i = 0; i < nkb; ++i) {
-      const int s = i % nst;
-      if (!mbar_wait(&full_bar[s], (i / nst) & 1, abort)) break;
-      tcgen05_fence_after();
-      const uint32_t abase = sbase + uint32_t(s) * sbytes, bbase = abase + 4u * a_ps;
-#pragma unroll
-      for (int c = 0; c < 12; ++c) {
-        const uint64_t ad = smem_desc(abase + uint32_t(kCombo[c][0]) * a_ps, 128u, a_sbo);
-        const uint64_t bd = smem_desc(bbase + uint32_t(kCombo[c][1]) * b_ps, 128u, b_sbo);
-        mma_bf16(tmem + (kCombo[c][2] ? ci_off : 0u), ad, bd, kCombo[c][3] ? id_neg : id_pos,
-                 i > 0 || (c != 0 && c != 6));
-      }
-      mma_commit(&empty_bar[s]);
-    }
-    mma_commit(&accum_bar);   // also on abort: arrives once every issued MMA has completed
   }
   tcgen05_fence_before();
   __syncthreads();
-  if (warp == kProdWarps) {
+  if (warp == kMmaWarp) {
     tcgen05_fence_after();
     tmem_dealloc(tmem, tcols);
   }
@@ -603,16 +425,23 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     tune_token = Tuner::begin(key, idx, st);
   }
   const int nt = (N + bn - 1) / bn;
-  // Dense operands are split once into bf16 planes in global memory by a
-  // bandwidth-bound pass; the GEMM then feeds its stages by bulk copies.
-  // Generated projector operands keep their in-kernel producers.
+  // Operands not given as planes are split into bf16 planes in global memory
+  // by a bandwidth-bound pass; the GEMM feeds its stages by bulk copies.
   TcOperand Ak = A, Bk = B;
   Profile& pf = rt.prof;
   int span0 = -1;
   if (nkb > 0) {
-    auto dense = [](const TcOperand& o) { return o.kind == TcOperand::kDenseK || o.kind == TcOperand::kDenseMN; };
     const int rpa = mt * kBM, rpb = nt * bn;
-    const long long pa = dense(A) ? (long long)rpa * nkb * 32 : 0, pb = dense(B) ? (long long)rpb * nkb * 32 : 0;
+    auto check = [&](const TcOperand& o, int rp, const char* which) {
+      if (o.kind == TcOperand::kPlanes &&
+          (o.planes == nullptr || o.rows_pad < rp || o.rows_pad % 16 != 0 || o.kdim != K ||
+           o.plane_bytes < (long long)o.rows_pad * nkb * 32 || (reinterpret_cast<uintptr_t>(o.planes) & 15) != 0))
+        fail(kInvalidArgument, std::string("pre-split ") + which + " operand does not cover the product");
+    };
+    check(A, rpa, "A");
+    check(B, rpb, "B");
+    const long long pa = A.kind != TcOperand::kPlanes ? (long long)rpa * nkb * 32 : 0;
+    const long long pb = B.kind != TcOperand::kPlanes ? (long long)rpb * nkb * 32 : 0;
     if (pa + pb > 0) {
       const size_t bytes = size_t(4) * size_t(pa + pb);
       if (rt.tc_planes.size() < bytes) rt.tc_planes.resize(bytes);
@@ -645,7 +474,7 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
       HALF_LAUNCH("tensor-core operand split");
     }
   }
-  const size_t sbytes = stage_bytes(bn, Ak.kind, Bk.kind);
+  const size_t sbytes = stage_bytes(bn);
   const int nst = int(std::min<size_t>(kMaxPipe, (kSmemBudget - kSmemSlack) / sbytes));
   if (nst < 2) fail(kInternal, "tensor-core GEMM stage does not fit shared memory twice");
   const size_t smem = size_t(nst) * sbytes + kSmemSlack;
@@ -693,6 +522,26 @@ void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N,
     HALF_LAUNCH("split-K reduction");
     ++rt.prof.launches;
   }
+}
+
+TcOperand tc_presplit_a(Runtime& rt, const TcOperand& op, DeviceBuffer<unsigned char>& store) {
+  if (op.kind == TcOperand::kPlanes) fail(kInvalidArgument, "operand is already split");
+  const int rows_pad = (op.rows + kBM - 1) / kBM * kBM, nkb = (op.kdim + kBK - 1) / kBK;
+  const long long pbytes = (long long)rows_pad * nkb * 32;
+  TcOperand o;
+  o.kind = TcOperand::kPlanes;
+  o.rows = op.rows;
+  o.kdim = op.kdim;
+  o.rows_pad = rows_pad;
+  o.plane_bytes = pbytes;
+  if (pbytes == 0) return o;
+  if (store.size() < size_t(4 * pbytes)) store.resize(size_t(4 * pbytes));
+  presplit_kernel<<<ceil_div((long long)rows_pad * nkb * 2, 256), 256, 0, rt.stream>>>(op, rows_pad, nkb, store.get(),
+                                                                                       pbytes);
+  HALF_LAUNCH("tensor-core operand split (kept)");
+  ++rt.prof.launches;
+  o.planes = store.get();
+  return o;
 }
 
 void tc_check(Runtime& rt) {

@@ -4,9 +4,10 @@
 // Every operand element is split into bf16 planes, x = x_hi + x_lo
 // (x_hi = bf16(x), x_lo = bf16(x - x_hi)), and each real product is taken as
 // x_hi y_hi + x_hi y_lo + x_lo y_hi with FP32 accumulation in Tensor Memory
-// (relative error about 2^-16).  Operands are either dense complex FP32
-// matrices or the projector matrix B of a k point generated in-tile from its
-// radial-angular table, plane-wave indices and atom phases (no stored B).
+// (relative error about 2^-16).  Operands are dense complex FP32 matrices,
+// the projector matrix B of a k point generated from its radial-angular
+// table, plane-wave indices and atom phases, or planes split beforehand
+// (tc_presplit_a) and reused across products.
 #pragma once
 
 #include <climits>
@@ -21,7 +22,7 @@ struct TcOperand {
     kDenseMN = 1,     // element (r, k) at p[r + k ld]: r contiguous
     kProjConj = 2,    // conj(B[g = k, col = r]): rows = projector columns, k = plane waves
     kProj = 3,        // B[g = r, col = k]: rows = plane waves, k = projector columns
-    kPlanes = 4       // pre-split bf16 planes in global memory (set up by tc_cgemm itself)
+    kPlanes = 4       // pre-split bf16 planes in global memory (tc_presplit_a, or tc_cgemm itself)
   };
   int kind = kDenseK;
   int rows = 0, kdim = 0;
@@ -52,6 +53,11 @@ TcOperand tc_dense_b(cublasOperation_t op, const float2* B, long long ldb, int K
 // With C2 set, output columns j >= split_col go to C2 column j - split_col (same ldc).
 void tc_cgemm(Runtime& rt, const TcOperand& A, const TcOperand& B, int M, int N, int K, double2 alpha,
               double2 beta, void* C, bool c_fp64, long long ldc, void* C2 = nullptr, int split_col = INT_MAX);
+
+// Splits `op`, used as the A operand of later products (M = op.rows,
+// K = op.kdim), into bf16 planes in `store` (grown when too small) and
+// returns the kPlanes operand that reads them; asynchronous on rt.stream.
+TcOperand tc_presplit_a(Runtime& rt, const TcOperand& op, DeviceBuffer<unsigned char>& store);
 
 // Raises kInternal if a tensor-core GEMM on this runtime gave up on a pipeline
 // wait (synchronises the stream).
