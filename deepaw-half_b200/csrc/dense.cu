@@ -12,6 +12,7 @@
 
 #include "blas.h"
 #include "context.h"
+#include "eig.h"
 
 namespace hb {
 
@@ -180,9 +181,16 @@ int read_info(const DeviceBuffer<int>& info, cudaStream_t st) {
 
 // Eigenvalues (and, with vectors, eigenvectors in place) of the Hermitian
 // matrix A through the 64-bit API; with index_range only the lowest nbands.
+// Without vectors the lowest nbands come from the tridiagonal route of
+// eig.cu instead: the 64-bit syevd's workspace query answered INVALID_VALUE
+// at the 216-atom cell's Gamma point (n = 38,089), as the 32-bit one did.
 void heevd64(Runtime& rt, const DnParams& prm, Work64& ws, bool vectors, bool index_range, long long n, int nbands,
              double2* A, double* w, DeviceBuffer<int>& info) {
-  const cusolverEigMode_t jobz = vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+  if (!vectors) {
+    hermitian_eigenvalues_large(rt, A, n, {0}, {nbands}, w);
+    return;
+  }
+  const cusolverEigMode_t jobz = CUSOLVER_EIG_MODE_VECTOR;
   size_t dbytes = 0, hbytes = 0;
   if (index_range) {
     double vl = 0, vu = 0;
@@ -222,13 +230,12 @@ void solve_dense_64(Runtime& rt, long long n, int nbands, bool index_range, bool
     // overlap extremes from the eigenvalues of S (src/half_cuda_solver.cuf:146-150)
     DeviceBuffer<double2> s2((size_t)n * n);
     HALF_CUDA(cudaMemcpyAsync(s2.get(), s, (size_t)n * n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-    heevd64(rt, prm, ws, false, false, n, nbands, s2.get(), w, info);
-    double lo = 0, hi = 0;
-    HALF_CUDA(cudaMemcpyAsync(&lo, w, sizeof(double), cudaMemcpyDeviceToHost, st));
-    HALF_CUDA(cudaMemcpyAsync(&hi, w + n - 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    hermitian_eigenvalues_large(rt, s2.get(), n, {0, int(n - 1)}, {1, 1}, w);
+    double ext[2] = {0, 0};
+    HALF_CUDA(cudaMemcpyAsync(ext, w, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     HALF_CUDA(cudaStreamSynchronize(st));
-    out.overlap_min = lo;
-    out.overlap_max = hi;
+    out.overlap_min = ext[0];
+    out.overlap_max = ext[1];
   } else {
     out.overlap_min = -1.0;
     out.overlap_max = -1.0;

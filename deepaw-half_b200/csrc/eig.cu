@@ -638,6 +638,43 @@ __global__ void __launch_bounds__(512) hetrd_kernel(double2* __restrict__ A, int
   }
 }
 
+// Large orders (the dense solves): T stays in global memory, read through
+// L1 with all lanes of a warp at the same index.  e2[i] = e[i]^2 and the
+// Gershgorin bounds (lo, hi, norm) are formed once by the first kernel.
+__global__ void tridiag_bounds_kernel(const double* __restrict__ d, const double* __restrict__ e, int n,
+                                      double* __restrict__ e2, double* __restrict__ bounds) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) e2[i] = i < n - 1 ? e[i] * e[i] : 0.0;
+  if (threadIdx.x == 0) gershgorin(d, e, n, bounds[0], bounds[1], bounds[2]);
+}
+
+// Eigenvalues k0 .. k0 + ne - 1 of T (ascending), one warp each, by the same
+// multisection as tridiag_values_kernel.
+__global__ void __launch_bounds__(32 * kValueWarps) tridiag_values_global_kernel(const double* __restrict__ d,
+                                                                                 const double* __restrict__ e2, int n,
+                                                                                 int k0, int ne,
+                                                                                 const double* __restrict__ bounds,
+                                                                                 double* __restrict__ lam) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * kValueWarps + (threadIdx.x >> 5);
+  if (j >= ne) return;
+  const int k = k0 + j;
+  const double tnorm = bounds[2];
+  double lo = bounds[0], hi = bounds[1];
+  for (int round = 0; round < 200; ++round) {
+    if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + DBL_EPSILON * tnorm) break;
+    const double x = lo + (hi - lo) * double(lane + 1) / 33.0;
+    const unsigned b = __ballot_sync(0xffffffffu, sturm_count(d, e2, n, x) > k);
+    const int first = b ? __ffs(b) - 1 : 32;
+    const double xlo = __shfl_sync(0xffffffffu, x, first > 0 ? first - 1 : 0);
+    const double xhi = __shfl_sync(0xffffffffu, x, first < 32 ? first : 31);
+    const double nlo = first > 0 ? xlo : lo, nhi = first < 32 ? xhi : hi;
+    if (!(nlo > lo || nhi < hi)) break;
+    lo = nlo;
+    hi = nhi;
+  }
+  if (lane == 0) lam[j] = 0.5 * (lo + hi);
+}
+
 }  // namespace
 
 void SmallEigen::reserve(Runtime& rt, int nmax) {
@@ -768,6 +805,43 @@ bool SmallEigen::metric_normalize(Runtime& rt, double2* M, int m, int* status) {
   HALF_LAUNCH("metric factor");
   rt.prof.launches += 1;
   return true;
+}
+
+void hermitian_eigenvalues_large(Runtime& rt, double2* A, long long n, const std::vector<int>& k0s,
+                                 const std::vector<int>& counts, double* lam) {
+  if (n > INT32_MAX / 2) fail(kUnavailable, "dense order beyond the tridiagonalisation's range");
+  cudaStream_t s = rt.stream;
+  const int ni = int(n);
+  DeviceBuffer<double> d(ni), e(ni), e2(ni), bounds(3);
+  DeviceBuffer<double2> tau(ni);
+  DeviceBuffer<int> info(1);
+  int lwork = 0;
+  cusolver_check(cusolverDnZhetrd_bufferSize(rt.solver, CUBLAS_FILL_MODE_UPPER, ni,
+                                             reinterpret_cast<cuDoubleComplex*>(A), ni, d.get(), e.get(),
+                                             reinterpret_cast<cuDoubleComplex*>(tau.get()), &lwork),
+                 "zhetrd buffer (large)");
+  DeviceBuffer<double2> work(size_t(std::max(lwork, 1)));
+  cusolver_check(cusolverDnZhetrd(rt.solver, CUBLAS_FILL_MODE_UPPER, ni, reinterpret_cast<cuDoubleComplex*>(A), ni,
+                                  d.get(), e.get(), reinterpret_cast<cuDoubleComplex*>(tau.get()),
+                                  reinterpret_cast<cuDoubleComplex*>(work.get()), lwork, info.get()),
+                 "zhetrd (large)");
+  int hinfo = 0;
+  HALF_CUDA(cudaMemcpyAsync(&hinfo, info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  HALF_CUDA(cudaStreamSynchronize(s));
+  if (hinfo != 0) fail(kInternal, "Householder tridiagonalisation failed");
+  tridiag_bounds_kernel<<<1, 1024, 0, s>>>(d.get(), e.get(), ni, e2.get(), bounds.get());
+  HALF_LAUNCH("tridiagonal bounds");
+  int off = 0;
+  for (size_t r = 0; r < k0s.size(); ++r) {
+    const int k0 = k0s[r], ne = counts[r];
+    if (k0 < 0 || ne < 0 || k0 + ne > ni) fail(kInvalidArgument, "eigenvalue index range outside the matrix");
+    if (ne == 0) continue;
+    tridiag_values_global_kernel<<<ceil_div(ne, kValueWarps), 32 * kValueWarps, 0, s>>>(d.get(), e2.get(), ni, k0, ne,
+                                                                                       bounds.get(), lam + off);
+    HALF_LAUNCH("tridiagonal eigenvalues (large)");
+    off += ne;
+  }
+  HALF_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace hb

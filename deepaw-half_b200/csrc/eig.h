@@ -1,6 +1,8 @@
 // Device-resident small Hermitian eigensolvers (see eig.cu).
 #pragma once
 
+#include <vector>
+
 #include "context.h"
 
 namespace hb {
@@ -24,5 +26,13 @@ struct SmallEigen {
   // (P U)^H S (P U) = I; returns false (nothing launched) when m is too large.
   bool metric_normalize(Runtime& rt, double2* M, int m, int* status);
 };
+
+// Selected eigenvalues of a large Hermitian matrix A (n x n, column-major,
+// upper triangle used and destroyed): Householder tridiagonalisation
+// (cuSOLVER zhetrd), then multisection on Sturm counts for the index ranges
+// [k0s[r], k0s[r] + counts[r]), written one range after another to lam
+// (device).  Synchronises the stream.
+void hermitian_eigenvalues_large(Runtime& rt, double2* A, long long n, const std::vector<int>& k0s,
+                                 const std::vector<int>& counts, double* lam);
 
 }  // namespace hb

@@ -53,7 +53,7 @@ def test_apply_hs_fp64(name, k, si2, hfo2, oracle_system):
 @pytest.mark.parametrize("k", [(0, 0, 0), (0.125, -0.25, 0.375)])
 def test_apply_hs_fp32(name, k, si2, hfo2, oracle_system):
     """The mixed mode's operator: FP32 local part, projector part on the
-    tensor cores with B generated in-tile (split bf16, 2^-16).  H psi and S psi
+    tensor cores with B split into bf16 planes once per k point (2^-16).  H psi and S psi
     agree with the FP64 oracle to 1e-4 of their largest element, and the
     projector part alone (S psi - psi = B Q B^H psi) to 1e-4 of its own."""
     from oracle import hamiltonian as H
@@ -234,10 +234,13 @@ def test_guarded_and_mixed_match_dense_on_the_64_atom_cell(inputs_dir):
 
 @pytest.mark.parametrize("solver,nb", [("evd", 16), ("vasp", 8)])
 def test_dense_64bit_path_matches_oracle(solver, nb, si2, oracle_system, monkeypatch):
-    """Large orders (above 16,384 plane waves) solve through the 64-bit solver API
-    (Cholesky, two triangular solves, Hermitian evd); HALF_DENSE_64BIT_ORDER=0
-    sends this small cell down that path, which must give the oracle's
-    eigenpairs, overlap extremes and S-normalisation like the 32-bit path."""
+    """Large orders (above 16,384 plane waves) solve through the 64-bit solver API:
+    Cholesky and two triangular solves, then for eigenvalues alone (and the
+    overlap extremes) Householder tridiagonalisation with multisection on
+    Sturm counts, for eigenpairs the 64-bit Hermitian evd.
+    HALF_DENSE_64BIT_ORDER=0 sends this small cell down that path, which must
+    give the oracle's eigenpairs, overlap extremes and S-normalisation like the
+    32-bit path."""
     from oracle import hamiltonian as H
     op = H.prepare(oracle_system("si2", si2))
     w, _, smin, smax = H.solve_dense(op, nb)
