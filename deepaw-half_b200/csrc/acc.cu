@@ -149,6 +149,35 @@ __global__ void scale_columns_kernel(double2* u, int m, const double* mu, double
   u[t] = cscale(u[t], 1.0 / sqrt(fmax(mu[j], floor_value)));
 }
 
+// Jacobi scaling of an order-n pencil (H, S): d[i] = 1 / sqrt(Re S(i,i))
+// (1 where that is not positive) by the first kernel, then H(i,j) and S(i,j)
+// times d[i] d[j] by the second.
+__global__ void jacobi_diag_kernel(const double2* __restrict__ s, int n, double* __restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double si = s[(long long)i * n + i].x;
+  d[i] = si > 0.0 ? 1.0 / sqrt(si) : 1.0;
+}
+
+__global__ void jacobi_scale_kernel(double2* __restrict__ h, double2* __restrict__ s, int n,
+                                    const double* __restrict__ d) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * n) return;
+  const int i = int(t % n), j = int(t / n);
+  const double f = d[i] * d[j];
+  h[t] = cscale(h[t], f);
+  s[t] = cscale(s[t], f);
+}
+
+// Y(i, j) *= d[i] for the first `cols` columns (eigenvectors of the scaled
+// pencil back to the unscaled one).
+__global__ void scale_rows_kernel(double2* __restrict__ y, int ld, int rows, int cols, const double* __restrict__ d) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)rows * cols) return;
+  const int i = int(t % rows), j = int(t / rows);
+  y[(long long)j * ld + i] = cscale(y[(long long)j * ld + i], d[i]);
+}
+
 template <typename A, typename B>
 __global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -219,10 +248,14 @@ struct SmallSolver {
   DeviceBuffer<int> info;   // [0] metric heevd, [1] RR hegvd, [2] RR Cholesky (own solver)
   int lw_ev = 0, lw_gv = 0;
   bool own = true;
+  // cuSOLVER pencils: only the nev lowest pairs (zhegvdx, index range; the
+  // default) or all of them (zhegvd, HALF_PENCIL_RANGE=0)
+  bool range = true;
   SmallEigen eig;
   SmallSolver(Runtime& r, int m_, double2* a, double2* b, double* w) : rt(r), m(m_) {
     const char* sel = std::getenv("HALF_SMALL_EIG");
     own = !(sel && std::string(sel) == "cusolver");
+    if (const char* pr = std::getenv("HALF_PENCIL_RANGE")) range = std::string(pr) != "0";
     info.resize(3);
     info.zero(rt.stream);
     if (own && 2 * m <= SmallEigen::kOwnMaxOrder) eig.reserve(rt, 2 * m);
@@ -238,7 +271,19 @@ struct SmallSolver {
                                                CUBLAS_FILL_MODE_UPPER, m, reinterpret_cast<cuDoubleComplex*>(a), m,
                                                reinterpret_cast<cuDoubleComplex*>(b), m, w, &l3),
                    "zhegvd buffer");
-    work.resize(size_t(std::max({l1, l2, l3, 1})));
+    int l4 = 0, l5 = 0, meig = 0;
+    cusolver_check(cusolverDnZhegvdx_bufferSize(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, 2 * m,
+                                                reinterpret_cast<cuDoubleComplex*>(a), 2 * m,
+                                                reinterpret_cast<cuDoubleComplex*>(b), 2 * m, 0.0, 0.0, 1, m, &meig, w,
+                                                &l4),
+                   "zhegvdx buffer");
+    cusolver_check(cusolverDnZhegvdx_bufferSize(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                CUSOLVER_EIG_RANGE_I, CUBLAS_FILL_MODE_UPPER, m,
+                                                reinterpret_cast<cuDoubleComplex*>(a), m,
+                                                reinterpret_cast<cuDoubleComplex*>(b), m, 0.0, 0.0, 1, m, &meig, w, &l5),
+                   "zhegvdx buffer");
+    work.resize(size_t(std::max({l1, l2, l3, l4, l5, 1})));
     lw_ev = l1;
     lw_gv = std::max(l2, l3);
   }
@@ -253,6 +298,16 @@ struct SmallSolver {
   // generalized problem of order n; the nev lowest eigenvectors are wanted
   void hegvd(double2* a, double2* b, int n, double* w, int nev) {
     if (own && n <= SmallEigen::kOwnMaxOrder) { eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2); return; }
+    if (range) {
+      int meig = 0;   // the routine returns it through host memory (it synchronises the stream)
+      cusolver_check(cusolverDnZhegvdx(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
+                                       CUBLAS_FILL_MODE_UPPER, n, reinterpret_cast<cuDoubleComplex*>(a), n,
+                                       reinterpret_cast<cuDoubleComplex*>(b), n, 0.0, 0.0, 1, nev, &meig, w,
+                                       reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()),
+                                       info.get() + 1),
+                     "zhegvdx");
+      return;
+    }
     cusolver_check(cusolverDnZhegvd(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
                                     n, reinterpret_cast<cuDoubleComplex*>(a), n, reinterpret_cast<cuDoubleComplex*>(b),
                                     n, w, reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()),
@@ -290,7 +345,7 @@ struct Blocks {
 
 struct Scratch64 {
   DeviceBuffer<double2> metric, hsub, ssub;   // m x m, 2m x 2m, 2m x 2m
-  DeviceBuffer<double> w, mu, norms, kinetic;
+  DeviceBuffer<double> w, mu, norms, kinetic, jacobi;
   DeviceBuffer<int> idx, active;
 };
 
@@ -328,6 +383,7 @@ struct AccRun {
   int n, m, chunk;
   int mcheck = m;              // bands whose residuals decide convergence (guard bands excluded)
   bool guarded = false;        // guard-band modes: may skip the separate metric normalisation
+  int metric_fallbacks = 0;    // Jacobi-scaled pencils whose Cholesky failed (redone with the metric step)
   double op_ms = 0;
   long long op_cols = 0;
   Tracer* tr = nullptr;
@@ -420,25 +476,55 @@ struct AccRun {
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, blk.hx(), n, blk.small.get(), m, one, blk.HP.get(), n);
     gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, np, m, mone, blk.sx(), n, blk.small.get(), m, one, blk.SP.get(), n);
     mark("orth_gemm");
-    // In the guard-band modes, when the library's own pencil solver takes
-    // the Rayleigh-Ritz step, the separate S-metric normalisation is
-    // skipped: that solver Jacobi-scales the overlap and floors dependent
-    // pivots exactly like the metric step, so [X P] spans the same space
-    // and the Ritz pairs are the same.  The FP64 mode keeps the reference's
-    // metric step.
+    // In the guard-band modes the separate S-metric normalisation is
+    // skipped.  The library's own pencil solver (small orders) Jacobi-scales
+    // the overlap and floors dependent pivots exactly like the metric step,
+    // so [X P] spans the same space and the Ritz pairs are the same.  Larger
+    // pencils go to cuSOLVER zhegvd Jacobi-scaled here, whose Cholesky of
+    // the overlap then does the metric step's work; if that Cholesky (or
+    // the solve) fails, the step is redone with the metric normalisation.
+    // The FP64 mode keeps the reference's metric step.
     const int ord = m + np;
-    const bool skip_metric = guarded && ss.own && ord <= SmallEigen::kOwnMaxOrder;
-    C* pu = skip_metric ? blk.P.get() : blk.PU.get();
-    C* hpu = skip_metric ? blk.HP.get() : blk.HPU.get();
-    C* spu = skip_metric ? blk.SP.get() : blk.SPU.get();
-    if (!skip_metric) normalise_metric(one, zero, np);
-    // Rayleigh-Ritz on Z = [X PU]
+    const bool own_pencil = ss.own && ord <= SmallEigen::kOwnMaxOrder;
+    bool skip_metric = guarded && ss.own;
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
+    C* pu = blk.P.get();
+    C* hpu = blk.HP.get();
+    C* spu = blk.SP.get();
+    auto use_metric = [&]() {
+      normalise_metric(one, zero, np);
+      pu = blk.PU.get();
+      hpu = blk.HPU.get();
+      spu = blk.SPU.get();
+    };
+    if (!skip_metric) use_metric();
+    // Rayleigh-Ritz on Z = [X PU]
     project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs);
     project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb);
     mark("rr_gemm");
-    ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+    if (skip_metric && !own_pencil) {
+      jacobi_diag_kernel<<<ceil_div(ord, 256), 256, 0, rt.stream>>>(ssb, ord, sc.jacobi.get());
+      jacobi_scale_kernel<<<ceil_div((long long)ord * ord, 256), 256, 0, rt.stream>>>(hs, ssb, ord, sc.jacobi.get());
+      HALF_LAUNCH("Jacobi scaling");
+      rt.prof.launches += 2;
+      ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+      int st = 0;
+      HALF_CUDA(cudaMemcpyAsync(&st, ss.info.get() + 1, sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
+      HALF_CUDA(cudaStreamSynchronize(rt.stream));
+      if (st == 0) {
+        scale_rows_kernel<<<ceil_div((long long)ord * m, 256), 256, 0, rt.stream>>>(hs, ord, ord, m, sc.jacobi.get());
+        ++rt.prof.launches;
+      } else {
+        ++metric_fallbacks;
+        use_metric();
+        project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs);
+        project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb);
+        ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+      }
+    } else {
+      ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+    }
     mark("hegvd");
     to_r(hs, ord, blk.Y.get(), ord, ord, m);
     const C* ytop = blk.Y.get();
@@ -504,6 +590,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   sc.hsub.resize(size_t(4) * m * m);
   sc.ssub.resize(size_t(4) * m * m);
   sc.w.resize(2 * m);
+  sc.jacobi.resize(2 * m);
   sc.mu.resize(m);
   sc.norms.resize(m);
   sc.kinetic.upload(ks.basis.kinetic, rt.stream);
@@ -539,6 +626,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   double op_ms = 0;
   long long op_cols = 0;
 
+  int fallbacks = 0;
   Blocks<double> b64;
   b64.allocate(n, m);
   DeviceBuffer<double2> tmp64(size_t(4) * m * m);
@@ -576,6 +664,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     if (iter > cfg.max_iter) iter = cfg.max_iter;
     op_ms += run32.op_ms;
     op_cols += run32.op_cols;
+    fallbacks += run32.metric_fallbacks;
     // promote X, recreate H X and S X in FP64, Rayleigh-Ritz
     convert_kernel<float2, double2><<<ceil_div((long long)n * m, 256), 256, 0, rt.stream>>>(b32.x(), b64.x(), (long long)n * m);
     ++rt.prof.launches;
@@ -605,6 +694,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   }
   op_ms += run64.op_ms;
   op_cols += run64.op_cols;
+  fallbacks += run64.metric_fallbacks;
   std::vector<double> w(2 * m);
   HALF_CUDA(cudaMemcpyAsync(w.data(), sc.w.get(), 2 * m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
   HALF_CUDA(cudaStreamSynchronize(rt.stream));
@@ -621,6 +711,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   }
   HALF_CUDA(cudaStreamSynchronize(rt.stream));
   tracer.report(iter);
+  if (tracer.on && fallbacks) std::fprintf(stderr, "HALF Jacobi-scaled pencils redone with the metric step: %d\n", fallbacks);
   info.iterations = iter;
   info.fp64_iterations = fp64_iter;
   info.converged = converged ? 1 : 0;

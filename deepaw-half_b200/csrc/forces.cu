@@ -6,16 +6,18 @@
 // atom and band, then
 //   F_I,alpha -= 2 w f_n Re[((D_I - eps_n Q) c)^H dc_alpha] + w f_n Re[c^H dD_I/dR_alpha c].
 //
-// B200 design: one kernel, one CTA per (atom, 32-band tile), 8 warps.  Per
+// B200 design: one kernel, one CTA per (atom, tile of 128 bands; 64 or 32
+// for atoms with more than 8 or 16 channels), 8 warps.  Per
 // chunk of 32 plane waves the CTA stages psi (coalesced along g), the plane
 // waves' q vectors, the atom's phase exp(+i q.R) (from the packed G indices and
 // the atom's b_j.R / 2 pi, reduced to one turn in FP64) and the chunk of
 // conj(B) = Omega^-1/2 beta_l(|q|) Y_lm(q^) i^l exp(+i q.R) generated from the
 // k point's radial-angular table: B is never stored, and neither is the
-// [psi | i q psi] block.  Lane = band, warp = a group of projector channels:
-// every thread accumulates c and u_alpha = sum_g q_alpha conj(B) psi in FP64
-// registers (dc_alpha = i u_alpha).  The epilogue contracts them with D, Q and
-// dD/dR per band and reduces the 32 bands with warp shuffles; a second kernel
+// [psi | i q psi] block.  Thread = (band, group of up to four projector
+// channels): every thread accumulates c and u_alpha = sum_g q_alpha conj(B)
+// psi for its channels in FP64 registers (dc_alpha = i u_alpha).  The
+// epilogue contracts them with D, Q and dD/dR per band and reduces the
+// tile's bands with warp shuffles and one ordered sum; a second kernel
 // adds the band tiles of each atom in order, so the result does not depend on
 // scheduling.  Bands with zero occupation are skipped as in the reference.
 #include <algorithm>
@@ -27,11 +29,9 @@ namespace hb {
 namespace {
 
 constexpr int kMaxNlm = 32;
-constexpr int kAdjBands = 32;                  // bands per CTA (the lanes)
-constexpr int kAdjGroups = 8;                  // projector-channel groups (the warps)
+constexpr int kAdjThreads = 256;
+constexpr int kAdjPer = 4;                     // projector channels per thread
 constexpr int kAdjG = 32;                      // plane waves per shared-memory chunk
-constexpr int kPerThread = kMaxNlm / kAdjGroups;
-constexpr int kAdjThreads = kAdjBands * kAdjGroups;
 
 struct AtomInfo {
   int col;     // first projector column of the atom
@@ -41,13 +41,23 @@ struct AtomInfo {
   int qofs;    // offset of the species Q
 };
 
-size_t adjoint_smem() {
-  const size_t chunk = (size_t(kAdjG) * kMaxNlm + size_t(kAdjG) * kAdjBands) * sizeof(double2) +
+// Shared memory of the kernel variant with BT bands per CTA (256 / BT
+// channel groups): the chunk staging, or the epilogue's c and dc of every
+// band of the tile, whichever is larger.
+size_t adjoint_smem(int bt) {
+  const int groups = kAdjThreads / bt;
+  const size_t chunk = (size_t(kAdjG) * kMaxNlm + size_t(kAdjG) * (bt + 1)) * sizeof(double2) +
                        size_t(kAdjG) * 4 * sizeof(double);
-  const size_t epilogue = size_t(4) * kAdjBands * kMaxNlm * sizeof(double2);
+  const size_t epilogue = size_t(4) * bt * groups * kAdjPer * sizeof(double2) + 8 * 3 * sizeof(double);
   return std::max(chunk, epilogue);
 }
 
+// One CTA per (atom, BT-band tile).  Thread = (band b = tid % BT, channel
+// group grp = tid / BT); it owns channels grp, grp + G, ... (up to kAdjPer of
+// them, G = 256 / BT groups, so atoms of up to 4 G channels).  A warp is 32
+// consecutive bands of one group: psi loads from shared memory are
+// conflict-free and the conj(B), q and phase loads are broadcasts.
+template <int BT>
 __global__ void __launch_bounds__(kAdjThreads)
     force_adjoint_kernel(const double2* __restrict__ psi, long long ld, int npw, int nb, const double* __restrict__ qv,
                          const double* __restrict__ ftab, const int* __restrict__ gpack, const int* __restrict__ pcol,
@@ -56,17 +66,22 @@ __global__ void __launch_bounds__(kAdjThreads)
                          const double* __restrict__ ddall, const double* __restrict__ qall,
                          const double* __restrict__ eig, const double* __restrict__ occ, double kweight,
                          double* __restrict__ partial) {
+  constexpr int G = kAdjThreads / BT;
+  constexpr int NL = G * kAdjPer;   // channel slots of a band in the epilogue
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* sB = reinterpret_cast<double2*>(smem_raw);      // [kAdjG][kMaxNlm]  conj(B)
-  double2* spsi = sB + kAdjG * kMaxNlm;                     // [kAdjG][kAdjBands]
-  double* sq = reinterpret_cast<double*>(spsi + kAdjG * kAdjBands);   // [kAdjG][4]: q_x, q_y, q_z
+  // [kAdjG][BT + 1]: the row pad keeps the g-major staging stores and the
+  // band-major reads free of bank conflicts
+  constexpr int BP = BT + 1;
+  double2* spsi = sB + kAdjG * kMaxNlm;
+  double* sq = reinterpret_cast<double*>(spsi + kAdjG * BP);   // [kAdjG][4]: q_x, q_y, q_z
   __shared__ double2 sph[kAdjG];
   __shared__ int sfrow[kMaxNlm], sl[kMaxNlm];
   const int ion = blockIdx.x, bt = blockIdx.y;
   const AtomInfo A = atoms[ion];
   const int nlm = A.nlm;
-  const int tid = threadIdx.x, nl = tid & 31, grp = tid >> 5;
-  const int n = bt * kAdjBands + nl;
+  const int tid = threadIdx.x, bl = tid % BT, grp = tid / BT;
+  const int n = bt * BT + bl;
   if (tid < nlm) {
     const int d = pcol[A.col + tid];
     sfrow[tid] = (d >> 2) & 0x3FFF;
@@ -74,11 +89,11 @@ __global__ void __launch_bounds__(kAdjThreads)
   }
   const int atom = pcol[A.col] >> 16;
   const double f0 = afrac[3 * atom], f1 = afrac[3 * atom + 1], f2 = afrac[3 * atom + 2];
-  double2 acc[4][kPerThread];
+  double2 acc[4][kAdjPer];
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int j = 0; j < kPerThread; ++j) acc[q][j] = make_double2(0.0, 0.0);
+    for (int j = 0; j < kAdjPer; ++j) acc[q][j] = make_double2(0.0, 0.0);
 
   for (int g0 = 0; g0 < npw; g0 += kAdjG) {
     __syncthreads();   // the previous chunk has been consumed
@@ -95,9 +110,9 @@ __global__ void __launch_bounds__(kAdjThreads)
       }
       sph[tid] = ph;
     }
-    for (int t = tid; t < kAdjG * kAdjBands; t += kAdjThreads) {
-      const int gl = t % kAdjG, b = t / kAdjG, g = g0 + gl, nn = bt * kAdjBands + b;
-      spsi[gl * kAdjBands + b] = (g < npw && nn < nb) ? psi[(long long)nn * ld + g] : make_double2(0.0, 0.0);
+    for (int t = tid; t < kAdjG * BT; t += kAdjThreads) {
+      const int gl = t % kAdjG, b = t / kAdjG, g = g0 + gl, nn = bt * BT + b;
+      spsi[gl * BP + b] = (g < npw && nn < nb) ? psi[(long long)nn * ld + g] : make_double2(0.0, 0.0);
     }
     for (int t = tid; t < kAdjG * 3; t += kAdjThreads) {
       const int gl = t / 3, a = t - 3 * gl, g = g0 + gl;
@@ -123,12 +138,13 @@ __global__ void __launch_bounds__(kAdjThreads)
     }
     __syncthreads();
     if (n < nb) {
+#pragma unroll 4
       for (int gl = 0; gl < kAdjG; ++gl) {
-        const double2 x = spsi[gl * kAdjBands + nl];
+        const double2 x = spsi[gl * BP + bl];
         const double qx = sq[4 * gl], qy = sq[4 * gl + 1], qz = sq[4 * gl + 2];
 #pragma unroll
-        for (int j = 0; j < kPerThread; ++j) {
-          const int a = grp + j * kAdjGroups;
+        for (int j = 0; j < kAdjPer; ++j) {
+          const int a = grp + j * G;
           if (a < nlm) {
             const double2 b = sB[gl * kMaxNlm + a];
             const double tr = b.x * x.x - b.y * x.y, ti = b.x * x.y + b.y * x.x;
@@ -147,56 +163,64 @@ __global__ void __launch_bounds__(kAdjThreads)
   }
   __syncthreads();
   // c and dc_alpha = i u_alpha of every band of the tile -> shared memory
-  double2* sc = reinterpret_cast<double2*>(smem_raw);   // [4][kAdjBands][kMaxNlm]
+  double2* sc = reinterpret_cast<double2*>(smem_raw);   // [4][BT][NL]
 #pragma unroll
-  for (int j = 0; j < kPerThread; ++j) {
-    const int a = grp + j * kAdjGroups;
+  for (int j = 0; j < kAdjPer; ++j) {
+    const int a = grp + j * G;
     if (a < nlm) {
-      sc[(0 * kAdjBands + nl) * kMaxNlm + a] = acc[0][j];
+      sc[(0 * BT + bl) * NL + a] = acc[0][j];
       for (int al = 0; al < 3; ++al)
-        sc[((1 + al) * kAdjBands + nl) * kMaxNlm + a] = make_double2(-acc[1 + al][j].y, acc[1 + al][j].x);
+        sc[((1 + al) * BT + bl) * NL + a] = make_double2(-acc[1 + al][j].y, acc[1 + al][j].x);
     }
   }
   __syncthreads();
-  if (tid >= 32) return;
-  double fsum[3] = {0.0, 0.0, 0.0};
-  const double fo = n < nb ? occ[n] : 0.0;
-  if (fo != 0.0) {
-    const double e = eig[n];
-    const double* D = dall + A.dofs;
-    const double* Q = qall + A.qofs;
-    const double2* c = sc + nl * kMaxNlm;
-    double2 mc[kMaxNlm];
-    for (int a = 0; a < nlm; ++a) {
-      double2 s = make_double2(0.0, 0.0);
-      for (int k = 0; k < nlm; ++k) {
-        const double w = D[a * nlm + k] - e * Q[a * nlm + k];
-        s.x += w * c[k].x;
-        s.y += w * c[k].y;
-      }
-      mc[a] = s;
-    }
-    for (int al = 0; al < 3; ++al) {
-      const double2* dc = sc + ((1 + al) * kAdjBands + nl) * kMaxNlm;
-      double re = 0.0;
-      for (int a = 0; a < nlm; ++a) re += mc[a].x * dc[a].x + mc[a].y * dc[a].y;   // Re(conj(mc) . dc)
-      const double* dD = ddall + A.ddofs + al * nlm * nlm;
-      double q = 0.0;
+  double* wsum = reinterpret_cast<double*>(sc + 4 * BT * NL);   // [BT / 32][3]
+  if (tid < BT) {
+    double fsum[3] = {0.0, 0.0, 0.0};
+    const double fo = n < nb ? occ[n] : 0.0;
+    if (fo != 0.0) {
+      const double e = eig[n];
+      const double* D = dall + A.dofs;
+      const double* Q = qall + A.qofs;
+      const double2* c = sc + bl * NL;
+      double2 mc[NL];
       for (int a = 0; a < nlm; ++a) {
         double2 s = make_double2(0.0, 0.0);
         for (int k = 0; k < nlm; ++k) {
-          s.x += dD[a * nlm + k] * c[k].x;
-          s.y += dD[a * nlm + k] * c[k].y;
+          const double w = D[a * nlm + k] - e * Q[a * nlm + k];
+          s.x += w * c[k].x;
+          s.y += w * c[k].y;
         }
-        q += c[a].x * s.x + c[a].y * s.y;   // Re(conj(c) . dD c)
+        mc[a] = s;
       }
-      fsum[al] = -2.0 * kweight * fo * re - kweight * fo * q;
+      for (int al = 0; al < 3; ++al) {
+        const double2* dc = sc + ((1 + al) * BT + bl) * NL;
+        double re = 0.0;
+        for (int a = 0; a < nlm; ++a) re += mc[a].x * dc[a].x + mc[a].y * dc[a].y;   // Re(conj(mc) . dc)
+        const double* dD = ddall + A.ddofs + al * nlm * nlm;
+        double q = 0.0;
+        for (int a = 0; a < nlm; ++a) {
+          double2 s = make_double2(0.0, 0.0);
+          for (int k = 0; k < nlm; ++k) {
+            s.x += dD[a * nlm + k] * c[k].x;
+            s.y += dD[a * nlm + k] * c[k].y;
+          }
+          q += c[a].x * s.x + c[a].y * s.y;   // Re(conj(c) . dD c)
+        }
+        fsum[al] = -2.0 * kweight * fo * re - kweight * fo * q;
+      }
+    }
+    for (int al = 0; al < 3; ++al) {
+      double v = fsum[al];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if ((tid & 31) == 0) wsum[(tid >> 5) * 3 + al] = v;
     }
   }
-  for (int al = 0; al < 3; ++al) {
-    double v = fsum[al];
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    if (tid == 0) partial[((long long)ion * gridDim.y + bt) * 3 + al] = v;
+  __syncthreads();
+  if (tid < 3) {   // the tile's warps in order
+    double v = 0.0;
+    for (int w = 0; w < BT / 32; ++w) v += wsum[w * 3 + tid];
+    partial[((long long)ion * gridDim.y + bt) * 3 + tid] = v;
   }
 }
 
@@ -240,7 +264,11 @@ void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec,
     ddall.insert(ddall.end(), ddh.begin(), ddh.end());
     col0 += sp.natoms * sp.nlm;
   }
-  const int ntiles = (nb + kAdjBands - 1) / kAdjBands;
+  int nlm_max = 1;
+  for (auto& sp : ctx.species) nlm_max = std::max(nlm_max, sp.nlm);
+  // bands per CTA: 128 for atoms of up to 8 channels, 64 up to 16, 32 up to 32
+  const int bt = nlm_max <= 2 * kAdjPer ? 128 : nlm_max <= 4 * kAdjPer ? 64 : 32;
+  const int ntiles = (nb + bt - 1) / bt;
   DeviceBuffer<AtomInfo> datoms;
   datoms.upload(atoms, st);
   DeviceBuffer<double> dd, ddd, dq, deig, docc, dpart(size_t(nions) * ntiles * 3), dout(size_t(nions) * 3);
@@ -249,13 +277,18 @@ void nonlocal_forces_device(Context& ctx, KOperatorSet& ks, const double2* dvec,
   dq.upload(qall, st);
   deig.upload(eig, nb, st);
   docc.upload(occ, nb, st);
-  const size_t smem = adjoint_smem();
-  raise_smem_limit(force_adjoint_kernel, smem);
+  const size_t smem = adjoint_smem(bt);
   Profile& pf = rt.prof;
   const int ev0 = pf.record(st);
-  force_adjoint_kernel<<<dim3(nions, ntiles), kAdjThreads, smem, st>>>(
-      dvec, ld, npw, nb, ks.qvec.get(), ks.ftab64.get(), ks.gpack.get(), ks.pcol.get(), ks.afrac.get(), ks.kf[0],
-      ks.kf[1], ks.kf[2], datoms.get(), dd.get(), ddd.get(), dq.get(), deig.get(), docc.get(), kweight, dpart.get());
+  auto launch = [&](auto kernel) {
+    raise_smem_limit(kernel, smem);
+    kernel<<<dim3(nions, ntiles), kAdjThreads, smem, st>>>(
+        dvec, ld, npw, nb, ks.qvec.get(), ks.ftab64.get(), ks.gpack.get(), ks.pcol.get(), ks.afrac.get(), ks.kf[0],
+        ks.kf[1], ks.kf[2], datoms.get(), dd.get(), ddd.get(), dq.get(), deig.get(), docc.get(), kweight, dpart.get());
+  };
+  if (bt == 128) launch(force_adjoint_kernel<128>);
+  else if (bt == 64) launch(force_adjoint_kernel<64>);
+  else launch(force_adjoint_kernel<32>);
   HALF_LAUNCH("force adjoint");
   sum_tiles_kernel<<<ceil_div(nions * 3, 128), 128, 0, st>>>(dpart.get(), nions, ntiles, dout.get());
   HALF_LAUNCH("force tiles");

@@ -107,37 +107,45 @@ __global__ void __launch_bounds__(512) k1_sphere_to_planes(const cplx_t<R>* __re
 template <typename R>
 __global__ void __launch_bounds__(256) k2_xlines(cplx_t<R>* __restrict__ work, int n1, int n2, int n3, int nplanes,
                                                  const int* __restrict__ plane_xpos, AxisPlan ax,
-                                                 const R* __restrict__ veff) {
+                                                 const R* __restrict__ veff, int nb, int bands_per_cta) {
+  // One CTA per (i2, z tile) and group of bands_per_cta of the chunk's nb
+  // bands, looping over its bands: the twiddles, the occupied-slot map and
+  // the tile's Veff are set up once per CTA.
   using C = cplx_t<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   C* X = tw + kMaxFFT;                                 // [i1][tz]
-  int* xpos = reinterpret_cast<int*>(X + n1 * kXTile);
+  R* vt = reinterpret_cast<R*>(X + n1 * kXTile);       // [i1][tz] Veff / N_r
+  int* xpos = reinterpret_cast<int*>(vt + n1 * kXTile);
   const int tiles = (n3 + kXTile - 1) / kXTile;
   const int i2 = blockIdx.x / tiles, z0 = (blockIdx.x - i2 * tiles) * kXTile;
   const int nz = min(kXTile, n3 - z0);
-  const int b = blockIdx.y;
   fill_twiddles(tw, n1);
-  for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) X[t] = czero<C>();
   for (int t = threadIdx.x; t < nplanes; t += blockDim.x) xpos[t] = plane_xpos[t];
-  __syncthreads();
-  const long long npl = (long long)n2 * n3;
-  C* base = work + (long long)b * nplanes * npl + (long long)i2 * n3 + z0;
-  for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
-    int jj = t / kXTile, c = t - jj * kXTile;
-    if (c < nz) X[xpos[jj] * kXTile + c] = base[jj * npl + c];
-  }
-  __syncthreads();
-  fft_pencils<true, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, +1);
   for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) {
-    int i1 = t / kXTile, c = t - i1 * kXTile;
-    if (c < nz) X[t] = cscale(X[t], veff[((long long)i1 * n2 + i2) * n3 + z0 + c]);
+    const int i1 = t / kXTile, c = t - i1 * kXTile;
+    vt[t] = c < nz ? veff[((long long)i1 * n2 + i2) * n3 + z0 + c] : R(0);
   }
-  __syncthreads();
-  fft_pencils<false, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, -1);
-  for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
-    int jj = t / kXTile, c = t - jj * kXTile;
-    if (c < nz) base[jj * npl + c] = X[xpos[jj] * kXTile + c];
+  const long long npl = (long long)n2 * n3;
+  const int bend = min(nb, (blockIdx.y + 1) * bands_per_cta);
+  for (int b = blockIdx.y * bands_per_cta; b < bend; ++b) {
+    for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) X[t] = czero<C>();
+    __syncthreads();
+    C* base = work + (long long)b * nplanes * npl + (long long)i2 * n3 + z0;
+    for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
+      int jj = t / kXTile, c = t - jj * kXTile;
+      if (c < nz) X[xpos[jj] * kXTile + c] = base[jj * npl + c];
+    }
+    __syncthreads();
+    fft_pencils<true, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, +1);
+    for (int t = threadIdx.x; t < n1 * kXTile; t += blockDim.x) X[t] = cscale(X[t], vt[t]);
+    __syncthreads();
+    fft_pencils<false, C, R>(X, kXTile, 1, kXTile, ax.plan, tw, -1);
+    for (int t = threadIdx.x; t < nplanes * kXTile; t += blockDim.x) {
+      int jj = t / kXTile, c = t - jj * kXTile;
+      if (c < nz) base[jj * npl + c] = X[xpos[jj] * kXTile + c];
+    }
+    __syncthreads();
   }
 }
 
@@ -318,7 +326,8 @@ size_t plane_smem(int n2, int n3) {
 }
 template <typename R>
 size_t xline_smem(int n1, int nplanes) {
-  return (kMaxFFT + size_t(n1) * kXTile) * sizeof(cplx_t<R>) + size_t(nplanes) * sizeof(int);
+  return (kMaxFFT + size_t(n1) * kXTile) * sizeof(cplx_t<R>) + size_t(n1) * kXTile * sizeof(R) +
+         size_t(nplanes) * sizeof(int);
 }
 
 struct HostGeom {
@@ -613,6 +622,9 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
   }
   const size_t psm = plane_smem<R>(op.n2, op.n3), xsm = xline_smem<R>(op.n1, op.nplanes);
   const int tiles = (op.n3 + kXTile - 1) / kXTile;
+  int sms = 148, dev = 0;
+  HALF_CUDA(cudaGetDevice(&dev));
+  HALF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   Profile& pf = rt.prof;
   const int ev_sweep = pf.record(s);
   const int ev_local = ev_sweep;
@@ -621,8 +633,12 @@ void apply_hs(Context& ctx, KOperatorSet& ks, const cplx_t<R>* x, long long ld, 
     k1_sphere_to_planes<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
         x, ld, b0, op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(), op.row_list.get(),
         op.ay, op.az, op.work.get());
-    k2_xlines<R><<<dim3(op.n2 * tiles, nbc), 256, xsm, s>>>(op.work.get(), op.n1, op.n2, op.n3, op.nplanes,
-                                                           op.plane_xpos.get(), op.ax, op.veff.get());
+    // bands per K2 CTA: as many as keep about eight CTAs per SM busy
+    const int lines = op.n2 * tiles;
+    const int groups = std::max(1, std::min(nbc, ceil_div(8 * sms, lines)));
+    const int bpc = ceil_div(nbc, groups);
+    k2_xlines<R><<<dim3(lines, ceil_div(nbc, bpc)), 256, xsm, s>>>(op.work.get(), op.n1, op.n2, op.n3, op.nplanes,
+                                                                  op.plane_xpos.get(), op.ax, op.veff.get(), nbc, bpc);
     k3_planes_to_sphere<R><<<dim3(op.nplanes, nbc), 512, psm, s>>>(
         op.work.get(), op.n2, op.n3, op.nplanes, op.plane_start.get(), op.spos.get(), op.row_start.get(),
         op.row_list.get(), op.ay, op.az, x, ld, b0, op.kinetic.get(), hx, sx);
@@ -728,7 +744,7 @@ void accumulate_band_density(KOperatorSet& ks, const double2* x, long long ld, i
     op.work_chunk = chunk;
   }
   const size_t psm = plane_smem<double>(op.n2, op.n3);
-  const size_t dsm = xline_smem<double>(op.n1, op.nplanes) + size_t(op.n1) * kXTile * sizeof(double);
+  const size_t dsm = xline_smem<double>(op.n1, op.nplanes);   // its accumulator takes the Veff tile's place
   raise_smem_limit(k2_density, dsm);
   const int tiles = (op.n3 + kXTile - 1) / kXTile;
   for (int b0 = 0; b0 < nb; b0 += chunk) {
