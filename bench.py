@@ -68,9 +68,10 @@ def parse():
     p.add_argument("--cpu-samples", type=int, default=3)
     p.add_argument("--no-check", action="store_true",
                    help="skip the dense FP64 reference eigenvalues (|d eps| reported as null)")
-    p.add_argument("--kernel", default=None, choices=["gemm"],
+    p.add_argument("--kernel", default=None, choices=["gemm", "forces"],
                    help="micro-benchmark one kernel on the workload's shapes instead of the solve (gemm: the "
-                        "tensor-core complex GEMM on the mixed phase's subspace shapes, synthetic operands)")
+                        "tensor-core complex GEMM on the mixed phase's subspace shapes, synthetic operands; "
+                        "forces: the FP64 force adjoint and one FP64 operator sweep on seeded bands)")
     p.add_argument("--reps", type=int, default=10, help="repetitions per shape of --kernel")
     p.add_argument("--quick", action="store_true",
                    help="only the timed mixed steps (profiling runs): no dense check, FP64 comparisons, e2e, "
@@ -322,6 +323,45 @@ def run_gemm_kernel(args):
                           "peak_source": kind, "workload": w.name}), flush=True)
 
 
+def run_forces_kernel(args):
+    """--kernel forces: the force adjoint (half_nonlocal_forces) and one FP64
+    H/S sweep (half_apply_hs) on the same seeded bands of the workload's first
+    k point (nbands columns; the adjoint's cost does not depend on the bands
+    being eigenvectors); device ms of each from the library's own events."""
+    import halfb200
+    from halfb200 import synth
+    w = synth.workload(args.workload)
+    ch, po = write_inputs(w, 0)
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
+        k = w.kpoints[0]
+        n = ctx.npw(k)
+        r = np.random.default_rng(3)
+        psi = (r.normal(size=(n, w.nbands)) + 1j * r.normal(size=(n, w.nbands))) / np.sqrt(2.0 * n)
+        eps = np.sort(r.uniform(-5.0, 5.0, size=w.nbands))
+        occ = np.where(np.arange(w.nbands) < int(w.nelect // 2), 2.0, 0.0)
+        ctx.set_acc(precision="fp64")
+        adj, sweep = [], []
+        for i in range(args.warmup + args.reps):
+            ctx.nonlocal_forces(k, psi, eps, occ, 1.0)
+            a = ctx.info()["adjoint_ms"]
+            ctx.apply_hs(k, psi)
+            sw = ctx.info()["sweep_ms"]
+            if i >= args.warmup:
+                adj.append(a)
+                sweep.append(sw)
+    a, sw = statistics.mean(adj), statistics.mean(sweep)
+    flops = 32.0 * n * ctx_np(w) * w.nbands
+    print(json.dumps({"kernel": "force_adjoint_kernel", "workload": w.name, "npw": n, "bands": w.nbands,
+                      "adjoint_ms": a, "sweep_ms_fp64": sw, "force_over_sweep": a / sw,
+                      "fp64_tflops_canonical": flops / (a * 1e-3) / 1e12,
+                      "flops_convention": "4 x 8 N_pw N_p m (c and three dc as complex products)"}), flush=True)
+
+
+def ctx_np(w):
+    """Projector columns of a workload: (2 l + 1) per channel per atom."""
+    return int(sum(cnt * sum(2 * l + 1 for l in sp.lps) for sp, cnt in zip(w.species, w.counts)))
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -330,6 +370,9 @@ def main():
         return
     if args.kernel == "gemm":
         run_gemm_kernel(args)
+        return
+    if args.kernel == "forces":
+        run_forces_kernel(args)
         return
     import halfb200
     from halfb200 import synth

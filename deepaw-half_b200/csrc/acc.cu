@@ -249,16 +249,22 @@ struct SmallSolver {
   int lw_ev = 0, lw_gv = 0;
   bool own = true;
   // cuSOLVER pencils: only the nev lowest pairs (zhegvdx, index range; the
-  // default) or all of them (zhegvd, HALF_PENCIL_RANGE=0)
+  // guard-band modes' default) or all of them (zhegvd: the FP64 mode, or
+  // HALF_PENCIL_RANGE=0)
   bool range = true;
+  // HALF_PENCIL_OWN=1: pencils above the own solver's order go through
+  // SmallEigen::hegv too (cuSOLVER zpotrf / zhetrd / zunmtr around the
+  // library's multisection and inverse-iteration kernels)
+  bool own_large = false;
   SmallEigen eig;
   SmallSolver(Runtime& r, int m_, double2* a, double2* b, double* w) : rt(r), m(m_) {
     const char* sel = std::getenv("HALF_SMALL_EIG");
     own = !(sel && std::string(sel) == "cusolver");
     if (const char* pr = std::getenv("HALF_PENCIL_RANGE")) range = std::string(pr) != "0";
+    if (const char* po = std::getenv("HALF_PENCIL_OWN")) own_large = own && std::string(po) != "0";
     info.resize(3);
     info.zero(rt.stream);
-    if (own && 2 * m <= SmallEigen::kOwnMaxOrder) eig.reserve(rt, 2 * m);
+    if (own && (2 * m <= SmallEigen::kOwnMaxOrder || own_large)) eig.reserve(rt, 2 * m);
     int l1 = 0, l2 = 0, l3 = 0;
     cusolver_check(cusolverDnZheevd_bufferSize(rt.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m,
                                                reinterpret_cast<cuDoubleComplex*>(a), m, w, &l1),
@@ -297,7 +303,10 @@ struct SmallSolver {
   }
   // generalized problem of order n; the nev lowest eigenvectors are wanted
   void hegvd(double2* a, double2* b, int n, double* w, int nev) {
-    if (own && n <= SmallEigen::kOwnMaxOrder) { eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2); return; }
+    if (own && (n <= SmallEigen::kOwnMaxOrder || own_large)) {
+      eig.hegv(rt, a, b, n, nev, w, info.get() + 1, info.get() + 2);
+      return;
+    }
     if (range) {
       int meig = 0;   // the routine returns it through host memory (it synchronises the stream)
       cusolver_check(cusolverDnZhegvdx(rt.solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUSOLVER_EIG_RANGE_I,
@@ -509,10 +518,10 @@ struct AccRun {
       HALF_LAUNCH("Jacobi scaling");
       rt.prof.launches += 2;
       ss.hegvd(hs, ssb, ord, sc.w.get(), m);
-      int st = 0;
-      HALF_CUDA(cudaMemcpyAsync(&st, ss.info.get() + 1, sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
+      int st[2] = {0, 0};   // solve status, Cholesky status (own solver)
+      HALF_CUDA(cudaMemcpyAsync(st, ss.info.get() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
       HALF_CUDA(cudaStreamSynchronize(rt.stream));
-      if (st == 0) {
+      if (st[0] == 0 && st[1] == 0) {
         scale_rows_kernel<<<ceil_div((long long)ord * m, 256), 256, 0, rt.stream>>>(hs, ord, ord, m, sc.jacobi.get());
         ++rt.prof.launches;
       } else {
@@ -598,6 +607,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   order.resize(m);
   sc.idx.upload(order, rt.stream);
   SmallSolver ss(rt, m, sc.hsub.get(), sc.ssub.get(), sc.w.get());
+  ss.range = ss.range && guarded;   // the FP64 mode keeps the reference's zhegvd
   const double seed_threshold = std::max(cfg.tol * 1e-2, 1e-12);
   std::vector<double> norms;
   // Soft locking (guard-band modes): a requested band whose residual is at or
@@ -651,7 +661,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run32.apply(b32.x(), b32.hx(), b32.sx(), m);
     run32.rayleigh_ritz_x();
     // Switch to FP64 once the residual is in the FP32 regime or stops improving.
-    const double switch_tol = std::max(cfg.tol, 3.0e-3);
+    // (HALF_FP32_SWITCH_EV overrides the 3e-3 eV switch point: measurement runs)
+    double switch_ev = 3.0e-3;
+    if (const char* sw = std::getenv("HALF_FP32_SWITCH_EV")) switch_ev = std::max(1e-8, std::atof(sw));
+    const double switch_tol = std::max(cfg.tol, switch_ev);
     double best = HUGE_VAL;
     int since_best = 0;
     for (iter = 1; iter <= cfg.max_iter; ++iter) {

@@ -638,6 +638,11 @@ __global__ void __launch_bounds__(512) hetrd_kernel(double2* __restrict__ A, int
   }
 }
 
+__global__ void real_to_complex_block_kernel(const double* __restrict__ z, long long count, double2* __restrict__ out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < count) out[t] = make_double2(z[t], 0.0);
+}
+
 // Large orders (the dense solves): T stays in global memory, read through
 // L1 with all lanes of a warp at the same index.  e2[i] = e[i]^2 and the
 // Gershgorin bounds (lo, hi, norm) are formed once by the first kernel.
@@ -699,7 +704,13 @@ void SmallEigen::reserve(Runtime& rt, int nmax) {
   cusolver_check(cusolverDnZpotrf_bufferSize(rt.solver, CUBLAS_FILL_MODE_UPPER, nmax,
                                              reinterpret_cast<cuDoubleComplex*>(V.get()), nmax, &l2),
                  "zpotrf buffer");
-  work.resize(size_t(std::max({l1, l2, 1})));
+  int l3 = 0;
+  cusolver_check(cusolverDnZunmtr_bufferSize(rt.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, nmax,
+                                             nmax, reinterpret_cast<cuDoubleComplex*>(V.get()), nmax,
+                                             reinterpret_cast<cuDoubleComplex*>(tau.get()),
+                                             reinterpret_cast<cuDoubleComplex*>(V.get()), nmax, &l3),
+                 "zunmtr buffer");
+  work.resize(size_t(std::max({l1, l2, l3, 1})));
 }
 
 // Hermitian eigenproblem of A (n x n, upper triangle used); the nev lowest
@@ -739,6 +750,22 @@ void SmallEigen::heev(Runtime& rt, double2* A, int n, int nev, double* w, int* s
   tridiag_vectors_kernel<<<ceil_div(nev, kVectorThreads), kVectorThreads, tsm, s>>>(d.get(), e.get(), n, nev, ne,
                                                                                      lam.get(), w, Z.get(), gs, status);
   HALF_LAUNCH("tridiagonal eigenvectors");
+  if (n > kMetricMax) {
+    // large orders: cuSOLVER's blocked back-transformation (zunmtr, Q Z with
+    // zhetrd's reflectors) on the complex copy of Z
+    real_to_complex_block_kernel<<<ceil_div((long long)n * nev, 256), 256, 0, s>>>(Z.get(), (long long)n * nev,
+                                                                                   V.get());
+    HALF_LAUNCH("tridiagonal eigenvectors to complex");
+    cusolver_check(cusolverDnZunmtr(rt.solver, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, n, nev,
+                                    reinterpret_cast<cuDoubleComplex*>(A), n,
+                                    reinterpret_cast<cuDoubleComplex*>(tau.get()),
+                                    reinterpret_cast<cuDoubleComplex*>(V.get()), n,
+                                    reinterpret_cast<cuDoubleComplex*>(work.get()), int(work.size()), info.get()),
+                   "zunmtr");
+    HALF_CUDA(cudaMemcpyAsync(A, V.get(), size_t(n) * nev * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    rt.prof.launches += 3;
+    return;
+  }
   // back-transformation: the reflectors in chunks that fit next to the warps' vectors
   const size_t vec_bytes = size_t(kBackWarps) * n * sizeof(double2);
   if (vec_bytes + (size_t(n) + 1) * sizeof(double2) > kSmemMax)
