@@ -178,6 +178,22 @@ __global__ void scale_rows_kernel(double2* __restrict__ y, int ld, int rows, int
   y[(long long)j * ld + i] = cscale(y[(long long)j * ld + i], d[i]);
 }
 
+// out[:, j] = in[:, perm[j]] for the m columns of an n-row block (ld n).
+template <typename C>
+__global__ void gather_columns_kernel(const C* __restrict__ in, C* __restrict__ out, int n, int m,
+                                      const int* __restrict__ perm) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)n * m) return;
+  const int j = int(t / n), i = int(t - (long long)j * n);
+  out[t] = in[(long long)perm[j] * n + i];
+}
+
+__global__ void gather_values_kernel(const double* __restrict__ in, double* __restrict__ out, int m,
+                                     const int* __restrict__ perm) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < m) out[j] = in[perm[j]];
+}
+
 template <typename A, typename B>
 __global__ void convert_kernel(const A* __restrict__ in, B* __restrict__ out, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -212,10 +228,15 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 struct Tracer {
   bool on = std::getenv("HALF_TRACE") != nullptr;
   bool history = on && std::string(std::getenv("HALF_TRACE")) == "2";   // per-iteration residuals
-  void step(const char* phase, int it, double res, const std::vector<double>& norms) {
+  // res: max residual over the requested bands; also the worst requested band
+  // and how many requested bands are at or below lock_tol (soft-locked)
+  void step(const char* phase, int it, double res, const std::vector<double>& norms, int mreq, double lock_tol) {
     if (!history) return;
-    int worst = int(std::max_element(norms.begin(), norms.end()) - norms.begin());
-    std::fprintf(stderr, "HALF iter %s %d %.6e band %d\n", phase, it, res, worst);
+    const int nr = std::min<int>(mreq, int(norms.size()));
+    int worst = int(std::max_element(norms.begin(), norms.begin() + nr) - norms.begin());
+    int locked = 0;
+    for (int j = 0; j < nr; ++j) locked += norms[j] <= lock_tol;
+    std::fprintf(stderr, "HALF iter %s %d %.6e band %d locked %d\n", phase, it, res, worst, locked);
   }
   cudaStream_t s = nullptr;
   std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
@@ -355,7 +376,7 @@ struct Blocks {
 struct Scratch64 {
   DeviceBuffer<double2> metric, hsub, ssub;   // m x m, 2m x 2m, 2m x 2m
   DeviceBuffer<double> w, mu, norms, kinetic, jacobi;
-  DeviceBuffer<int> idx, active;
+  DeviceBuffer<int> idx, active, perm;
 };
 
 // projected blocks into an ((m + np) x (m + np), ld m + np) FP64 matrix:
@@ -393,6 +414,9 @@ struct AccRun {
   int mcheck = m;              // bands whose residuals decide convergence (guard bands excluded)
   bool guarded = false;        // guard-band modes: may skip the separate metric normalisation
   int metric_fallbacks = 0;    // Jacobi-scaled pencils whose Cholesky failed (redone with the metric step)
+  int nl = 0;                  // hard-locked columns, at the front of X, H X, S X
+  std::vector<double> wh;      // Ritz values (host copy, physical column order)
+  std::vector<int> req;        // requested bands: physical columns of the mcheck lowest Ritz values
   double op_ms = 0;
   long long op_cols = 0;
   Tracer* tr = nullptr;
@@ -439,13 +463,17 @@ struct AccRun {
     blk.cur = nx;
   }
 
-  // residual norms of the current Ritz pairs; returns max norm (host sync)
+  // residual norms of the current Ritz pairs; returns the max norm over the
+  // requested bands, which are the mcheck lowest Ritz values (req, physical
+  // column indices in ascending order of their values; host sync)
   double residuals(std::vector<double>& norms, int* infos) {
     residual_norm_kernel<C><<<m, 256, 0, rt.stream>>>(blk.hx(), blk.sx(), n, n, sc.w.get(), sc.norms.get());
     ++rt.prof.launches;
     HALF_LAUNCH("residual norms");
     norms.resize(m);
+    wh.resize(m);
     HALF_CUDA(cudaMemcpyAsync(norms.data(), sc.norms.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
+    HALF_CUDA(cudaMemcpyAsync(wh.data(), sc.w.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
     ss.status_async(infos);
     HALF_CUDA(cudaStreamSynchronize(rt.stream));
     if constexpr (sizeof(R) == 4) tc_check(rt);
@@ -454,9 +482,68 @@ struct AccRun {
     if (infos[1] != 0) fail(kInternal, "ACC small generalized eigensolve failed (info " + std::to_string(infos[1]) + ")");
     if (infos[2] != 0)
       fail(kInternal, "ACC Rayleigh-Ritz overlap is not positive definite (Cholesky info " + std::to_string(infos[2]) + ")");
+    order_requested();
     double mx = 0;
-    for (int j = 0; j < mcheck && j < m; ++j) mx = std::max(mx, norms[j]);
+    for (int j : req) mx = std::max(mx, norms[j]);
     return mx;
+  }
+
+  // req from the host Ritz values wh: locked columns keep their values, so
+  // the physical order is ascending only without locking; a stable sort keeps
+  // it where it is
+  void order_requested() {
+    req.resize(m);
+    for (int j = 0; j < m; ++j) req[j] = j;
+    std::stable_sort(req.begin(), req.end(), [&](int a, int b) { return wh[a] < wh[b]; });
+    req.resize(std::min(mcheck, m));
+  }
+
+  // the current Ritz values to the host and req from them (after an iteration
+  // that no residual check followed: the iteration bound was reached)
+  void refresh_values() {
+    wh.resize(m);
+    HALF_CUDA(cudaMemcpyAsync(wh.data(), sc.w.get(), m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
+    HALF_CUDA(cudaStreamSynchronize(rt.stream));
+    order_requested();
+  }
+
+  // Hard locking: move the (unlocked) columns `newly` to the locked front
+  // [0, nl) of X, H X, S X, of the Ritz values and of the host norms; locked
+  // columns are no longer rotated or projected (their residuals stay as they
+  // were), and P stays S-orthogonal to them through the orthogonalisation
+  // against the whole of X.
+  void lock(const std::vector<int>& newly, std::vector<double>& norms) {
+    if (newly.empty()) return;
+    std::vector<char> is_new(m, 0);
+    for (int j : newly) is_new[j] = 1;
+    std::vector<int> perm;
+    perm.reserve(m);
+    for (int j = 0; j < nl; ++j) perm.push_back(j);
+    for (int j = nl; j < m; ++j)
+      if (is_new[j]) perm.push_back(j);
+    for (int j = nl; j < m; ++j)
+      if (!is_new[j]) perm.push_back(j);
+    sc.perm.upload(perm, rt.stream);
+    const int nx = blk.cur ^ 1;
+    const long long cnt = (long long)n * m;
+    gather_columns_kernel<C><<<ceil_div(cnt, 256), 256, 0, rt.stream>>>(blk.x(), blk.X[nx].get(), n, m, sc.perm.get());
+    gather_columns_kernel<C><<<ceil_div(cnt, 256), 256, 0, rt.stream>>>(blk.hx(), blk.HX[nx].get(), n, m, sc.perm.get());
+    gather_columns_kernel<C><<<ceil_div(cnt, 256), 256, 0, rt.stream>>>(blk.sx(), blk.SX[nx].get(), n, m, sc.perm.get());
+    gather_values_kernel<<<ceil_div(m, 256), 256, 0, rt.stream>>>(sc.w.get(), sc.mu.get(), m, sc.perm.get());
+    HALF_CUDA(cudaMemcpyAsync(sc.w.get(), sc.mu.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, rt.stream));
+    gather_values_kernel<<<ceil_div(m, 256), 256, 0, rt.stream>>>(sc.norms.get(), sc.mu.get(), m, sc.perm.get());
+    HALF_CUDA(cudaMemcpyAsync(sc.norms.get(), sc.mu.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, rt.stream));
+    HALF_LAUNCH("lock columns");
+    rt.prof.launches += 5;
+    blk.cur = nx;
+    std::vector<double> nn(m), ww(m);
+    for (int j = 0; j < m; ++j) {
+      nn[j] = norms[perm[j]];
+      ww[j] = wh[perm[j]];
+    }
+    norms.swap(nn);
+    wh.swap(ww);
+    nl += int(newly.size());
   }
 
   // one ACC iteration after the residual check (src/half_cuda_iterative_solver.cuf:158-195).
@@ -493,11 +580,16 @@ struct AccRun {
     // the overlap then does the metric step's work; if that Cholesky (or
     // the solve) fails, the step is redone with the metric normalisation.
     // The FP64 mode keeps the reference's metric step.
-    const int ord = m + np;
+    // Rayleigh-Ritz on Z = [X_U PU], X_U = the unlocked columns [nl, m) of X
+    // (all of them without hard locking)
+    const int mu = m - nl;
+    const long long off = (long long)nl * n;
+    const int ord = mu + np;
     const bool own_pencil = ss.own && ord <= SmallEigen::kOwnMaxOrder;
     bool skip_metric = guarded && ss.own;
     double2* hs = sc.hsub.get();
     double2* ssb = sc.ssub.get();
+    double* wu = sc.w.get() + nl;
     C* pu = blk.P.get();
     C* hpu = blk.HP.get();
     C* spu = blk.SP.get();
@@ -508,43 +600,50 @@ struct AccRun {
       spu = blk.SPU.get();
     };
     if (!skip_metric) use_metric();
-    // Rayleigh-Ritz on Z = [X PU]
-    project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs);
-    project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb);
+    auto project = [&]() {
+      project_upper<R>(rt, n, mu, np, blk.x() + off, pu, blk.hx() + off, hpu, hs);
+      project_upper<R>(rt, n, mu, np, blk.x() + off, pu, blk.sx() + off, spu, ssb);
+    };
+    project();
     mark("rr_gemm");
     if (skip_metric && !own_pencil) {
       jacobi_diag_kernel<<<ceil_div(ord, 256), 256, 0, rt.stream>>>(ssb, ord, sc.jacobi.get());
       jacobi_scale_kernel<<<ceil_div((long long)ord * ord, 256), 256, 0, rt.stream>>>(hs, ssb, ord, sc.jacobi.get());
       HALF_LAUNCH("Jacobi scaling");
       rt.prof.launches += 2;
-      ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+      ss.hegvd(hs, ssb, ord, wu, mu);
       int st[2] = {0, 0};   // solve status, Cholesky status (own solver)
       HALF_CUDA(cudaMemcpyAsync(st, ss.info.get() + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, rt.stream));
       HALF_CUDA(cudaStreamSynchronize(rt.stream));
       if (st[0] == 0 && st[1] == 0) {
-        scale_rows_kernel<<<ceil_div((long long)ord * m, 256), 256, 0, rt.stream>>>(hs, ord, ord, m, sc.jacobi.get());
+        scale_rows_kernel<<<ceil_div((long long)ord * mu, 256), 256, 0, rt.stream>>>(hs, ord, ord, mu, sc.jacobi.get());
         ++rt.prof.launches;
       } else {
         ++metric_fallbacks;
         use_metric();
-        project_upper<R>(rt, n, m, np, blk.x(), pu, blk.hx(), hpu, hs);
-        project_upper<R>(rt, n, m, np, blk.x(), pu, blk.sx(), spu, ssb);
-        ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+        project();
+        ss.hegvd(hs, ssb, ord, wu, mu);
       }
     } else {
-      ss.hegvd(hs, ssb, ord, sc.w.get(), m);
+      ss.hegvd(hs, ssb, ord, wu, mu);
     }
     mark("hegvd");
-    to_r(hs, ord, blk.Y.get(), ord, ord, m);
+    to_r(hs, ord, blk.Y.get(), ord, ord, mu);
     const C* ytop = blk.Y.get();
-    const C* ybot = blk.Y.get() + m;
+    const C* ybot = blk.Y.get() + mu;
     int nx = blk.cur ^ 1;
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.x(), n, ytop, ord, zero, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, pu, n, ybot, ord, one, blk.X[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.hx(), n, ytop, ord, zero, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, hpu, n, ybot, ord, one, blk.HX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, m, one, blk.sx(), n, ytop, ord, zero, blk.SX[nx].get(), n);
-    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, m, np, one, spu, n, ybot, ord, one, blk.SX[nx].get(), n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, mu, one, blk.x() + off, n, ytop, ord, zero, blk.X[nx].get() + off, n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, np, one, pu, n, ybot, ord, one, blk.X[nx].get() + off, n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, mu, one, blk.hx() + off, n, ytop, ord, zero, blk.HX[nx].get() + off, n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, np, one, hpu, n, ybot, ord, one, blk.HX[nx].get() + off, n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, mu, one, blk.sx() + off, n, ytop, ord, zero, blk.SX[nx].get() + off, n);
+    gemm(rt, CUBLAS_OP_N, CUBLAS_OP_N, n, mu, np, one, spu, n, ybot, ord, one, blk.SX[nx].get() + off, n);
+    if (nl > 0) {   // locked columns go along unchanged
+      const size_t bytes = size_t(off) * sizeof(C);
+      HALF_CUDA(cudaMemcpyAsync(blk.X[nx].get(), blk.x(), bytes, cudaMemcpyDeviceToDevice, rt.stream));
+      HALF_CUDA(cudaMemcpyAsync(blk.HX[nx].get(), blk.hx(), bytes, cudaMemcpyDeviceToDevice, rt.stream));
+      HALF_CUDA(cudaMemcpyAsync(blk.SX[nx].get(), blk.sx(), bytes, cudaMemcpyDeviceToDevice, rt.stream));
+    }
     blk.cur = nx;
     mark("rr_rot");
   }
@@ -621,6 +720,17 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   // FP64 mode, the reference's iteration, never locks.
   bool soft_lock = guarded;
   if (const char* sl = std::getenv("HALF_SOFT_LOCK")) soft_lock = guarded && std::string(sl) != "0";
+  // Hard locking (on with soft locking; HALF_HARD_LOCK=0 keeps the soft
+  // variant): a requested band at or below the lock tolerance leaves the
+  // iteration for the rest of the phase.  Its column moves to the locked
+  // front of X, H X, S X and is neither projected nor rotated again, so the
+  // pencils have order 2 (m - locked) and the rotations and projections
+  // shrink with them; P is still S-orthogonalised against the whole of X.
+  // On the 216-atom cell 235-470 of the 480 requested bands sit at or below
+  // the lock tolerance in most iterations of both phases.  Locks are
+  // released when the FP32 phase hands over to FP64.
+  bool hard_lock = soft_lock;
+  if (const char* hl = std::getenv("HALF_HARD_LOCK")) hard_lock = soft_lock && std::string(hl) != "0";
   std::vector<int> active;
   auto pick_active = [&](double lock_tol) -> const std::vector<int>* {
     if (!soft_lock) return nullptr;
@@ -628,6 +738,22 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     for (int j = 0; j < m; ++j)
       if (j >= mreq || !(norms[j] <= lock_tol)) active.push_back(j);
     return &active;
+  };
+  // one iteration of a phase: hard-lock the newly converged requested bands
+  // and iterate on the rest, or the soft-locked / reference step
+  auto advance = [&](auto& run, double lock_tol) {
+    if (!hard_lock) {
+      run.iterate(seed_threshold, pick_active(lock_tol));
+      return;
+    }
+    std::vector<int> newly;
+    for (int j : run.req)
+      if (j >= run.nl && norms[j] <= lock_tol && run.nl + int(newly.size()) + 1 < m) newly.push_back(j);
+    std::sort(newly.begin(), newly.end());
+    run.lock(newly, norms);
+    active.clear();
+    for (int j = run.nl; j < m; ++j) active.push_back(j);
+    run.iterate(seed_threshold, &active);
   };
   int infos[3] = {0, 0, 0};
   int iter = 0, fp64_iter = 0;
@@ -669,10 +795,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     int since_best = 0;
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run32.residuals(norms, infos);
-      tracer.step("fp32", iter, max_res, norms);
+      tracer.step("fp32", iter, max_res, norms, mreq, 0.5 * switch_tol);
       if (max_res < 0.9 * best) { best = max_res; since_best = 0; } else { ++since_best; }
       if (max_res <= switch_tol || since_best >= 6) break;
-      run32.iterate(seed_threshold, pick_active(0.5 * switch_tol));
+      advance(run32, 0.5 * switch_tol);
     }
     if (iter > cfg.max_iter) iter = cfg.max_iter;
     op_ms += run32.op_ms;
@@ -685,9 +811,9 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
       max_res = run64.residuals(norms, infos);
-      tracer.step("fp64", fp64_iter, max_res, norms);
+      tracer.step("fp64", fp64_iter, max_res, norms, mreq, 0.5 * cfg.tol);
       if (max_res <= cfg.tol) { converged = true; break; }
-      run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
+      advance(run64, 0.5 * cfg.tol);
     }
     fp64_iter = std::min(fp64_iter, cfg.max_iter);
     iter += fp64_iter;
@@ -698,9 +824,9 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run64.residuals(norms, infos);
-      tracer.step("fp64", iter, max_res, norms);
+      tracer.step("fp64", iter, max_res, norms, mreq, 0.5 * cfg.tol);
       if (max_res <= cfg.tol) { converged = true; break; }
-      run64.iterate(seed_threshold, pick_active(0.5 * cfg.tol));
+      advance(run64, 0.5 * cfg.tol);
     }
     iter = std::min(iter, cfg.max_iter);
     fp64_iter = iter;
@@ -708,19 +834,25 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   op_ms += run64.op_ms;
   op_cols += run64.op_cols;
   fallbacks += run64.metric_fallbacks;
-  std::vector<double> w(2 * m);
-  HALF_CUDA(cudaMemcpyAsync(w.data(), sc.w.get(), 2 * m * sizeof(double), cudaMemcpyDeviceToHost, rt.stream));
-  HALF_CUDA(cudaStreamSynchronize(rt.stream));
-  out.eigenvalues.assign(w.begin(), w.begin() + mreq);
+  // the requested eigenpairs in ascending order (req: physical columns, from
+  // the last residual check; the identity order unless bands were locked)
+  if (!converged) run64.refresh_values();   // the last step was an iteration, not a residual check
+  const std::vector<int>& req = run64.req;
+  if (int(req.size()) != mreq) fail(kInternal, "ACC finished without Ritz values");
+  out.eigenvalues.resize(mreq);
+  for (int i = 0; i < mreq; ++i) out.eigenvalues[i] = run64.wh[req[i]];
   out.overlap_min = -1.0;   // src/half_cuda_iterative_solver.cuf:200
   out.overlap_max = -1.0;
   out.dvectors.resize(size_t(n) * mreq);
-  HALF_CUDA(cudaMemcpyAsync(out.dvectors.get(), b64.x(), size_t(n) * mreq * sizeof(double2), cudaMemcpyDeviceToDevice,
-                            rt.stream));
+  sc.perm.upload(req, rt.stream);
+  gather_columns_kernel<double2><<<ceil_div((long long)n * mreq, 256), 256, 0, rt.stream>>>(
+      b64.x(), out.dvectors.get(), n, mreq, sc.perm.get());
+  HALF_LAUNCH("ACC output gather");
+  ++rt.prof.launches;
   if (want_vectors) {
     out.vectors.resize(size_t(2) * n * mreq);
-    HALF_CUDA(cudaMemcpyAsync(out.vectors.data(), b64.x(), size_t(n) * mreq * sizeof(double2), cudaMemcpyDeviceToHost,
-                              rt.stream));
+    HALF_CUDA(cudaMemcpyAsync(out.vectors.data(), out.dvectors.get(), size_t(n) * mreq * sizeof(double2),
+                              cudaMemcpyDeviceToHost, rt.stream));
   }
   HALF_CUDA(cudaStreamSynchronize(rt.stream));
   tracer.report(iter);

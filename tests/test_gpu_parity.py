@@ -261,28 +261,34 @@ def test_dense_64bit_path_matches_oracle(solver, nb, si2, oracle_system, monkeyp
 
 @pytest.mark.parametrize("name", ["si2", "hfo2"])
 def test_soft_locking_matches_dense(name, si2, hfo2, oracle_system, monkeypatch):
-    """Soft locking (the guard-band modes' default; HALF_SOFT_LOCK=0 turns it off): requested bands whose
-    residual is at or below half the tolerance add no correction direction, so
-    the Rayleigh-Ritz pencils shrink; the converged eigenvalues must still be
-    the dense solve's, and the operator must see fewer columns than without."""
+    """Locking in the guard-band modes (on by default; HALF_SOFT_LOCK=0 turns it
+    off).  Soft (HALF_HARD_LOCK=0): requested bands whose residual is at or
+    below half the tolerance add no correction direction, so the pencils shrink.
+    Hard (the default): such bands also leave the Rayleigh-Ritz step and the
+    rotations for the rest of the phase.  Either way the converged eigenvalues
+    must be the dense solve's, and the operator must see fewer columns than
+    without locking."""
     from oracle import hamiltonian as H
     files = {"si2": si2, "hfo2": hfo2}[name]
     w = files[0]
     op = H.prepare(oracle_system(name, files))
     nb = 8 if name == "si2" else w.nbands
     ref, _, _, _ = H.solve_dense(op, nb)
+    modes = {"off": ("0", "1"), "soft": ("1", "0"), "hard": ("1", "1")}
     with ctx_for(files) as ctx:
         for precision, tol in (("fp64_guarded", 1e-10), ("mixed", 1e-8)):
             cols = {}
-            for lock in ("0", "1"):
-                monkeypatch.setenv("HALF_SOFT_LOCK", lock)
+            for mode, (soft, hard) in modes.items():
+                monkeypatch.setenv("HALF_SOFT_LOCK", soft)
+                monkeypatch.setenv("HALF_HARD_LOCK", hard)
                 ctx.set_acc(tol=2e-5 if name == "hfo2" else 1e-7, max_iterations=400, precision=precision)
                 e, _, _, _ = ctx.solve((0, 0, 0), nb)
                 info = ctx.info()
-                assert info["converged"] == 1, (precision, lock)
-                assert np.abs(e - ref).max() <= tol, (precision, lock, np.abs(e - ref).max())
-                cols[lock] = info["operator_applications"] / max(1, info["iterations"])
-            assert cols["1"] < cols["0"], (precision, cols)
+                assert info["converged"] == 1, (precision, mode)
+                assert np.abs(e - ref).max() <= tol, (precision, mode, np.abs(e - ref).max())
+                assert np.all(np.diff(e) >= 0), (precision, mode)
+                cols[mode] = info["operator_applications"] / max(1, info["iterations"])
+            assert cols["soft"] < cols["off"] and cols["hard"] < cols["off"], (precision, cols)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
