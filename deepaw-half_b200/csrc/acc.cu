@@ -691,7 +691,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   // a higher level.  Convergence is decided on the requested bands only; the
   // FP64 mode is the reference algorithm unchanged (no guard bands).
   const bool guarded = mixed || cfg.precision == kFP64Guarded;
-  const int guard = guarded ? std::min(std::max(4, mreq / 8), n / 2 - mreq) : 0;
+  // (HALF_GUARD_DIV overrides the divisor 8 of m / 8: measurement runs)
+  int guard_div = 8;
+  if (const char* gd = std::getenv("HALF_GUARD_DIV")) guard_div = std::max(1, std::atoi(gd));
+  const int guard = guarded ? std::min(std::max(4, mreq / guard_div), n / 2 - mreq) : 0;
   const int m = mreq + guard;
   Scratch64 sc;
   sc.metric.resize(size_t(m) * m);
