@@ -29,7 +29,7 @@
 //   FP32 regime, then promotes X
 //   and finishes with FP64 iterations (one FP64 operator sweep re-creates
 //   H X and S X exactly before the first FP64 Rayleigh-Ritz); it carries
-//   m/8 (at least 4) guard bands and tests convergence on the requested m.
+//   m/4 (at least 4) guard bands and tests convergence on the requested m.
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
@@ -683,7 +683,7 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   if (2 * mreq > n) fail(kInvalidArgument, "ACC solver requires NBANDS <= NPL/2");
   const AccControls& cfg = ctx.acc;
   const bool mixed = cfg.precision == kMixed;
-  // The mixed and guarded modes carry guard bands (m/8, at least 4, within
+  // The mixed and guarded modes carry guard bands (m/4, at least 4, within
   // NPL/2): a requested edge band nearly degenerate with the first
   // unrequested one otherwise converges at the block method's edge rate
   // (after the FP32 phase up to ten times the FP64 iteration count), and a
@@ -691,8 +691,11 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   // a higher level.  Convergence is decided on the requested bands only; the
   // FP64 mode is the reference algorithm unchanged (no guard bands).
   const bool guarded = mixed || cfg.precision == kFP64Guarded;
-  // (HALF_GUARD_DIV overrides the divisor 8 of m / 8: measurement runs)
-  int guard_div = 8;
+  // m / 4 guard bands: on the 216-atom cell with hard locking, m/8, m/5, m/4,
+  // m/3 and m/2 gave 48, 31, 25, 22 and 17 iterations and 1.34, 1.18, 1.15,
+  // 1.19 and 1.23 s per k point (the extra columns cost more than the
+  // iterations they save beyond m/4).  HALF_GUARD_DIV overrides the divisor.
+  int guard_div = 4;
   if (const char* gd = std::getenv("HALF_GUARD_DIV")) guard_div = std::max(1, std::atoi(gd));
   const int guard = guarded ? std::min(std::max(4, mreq / guard_div), n / 2 - mreq) : 0;
   const int m = mreq + guard;

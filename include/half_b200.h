@@ -21,7 +21,7 @@ enum half_precision {
                                       guard bands */
   HALF_PRECISION_FP64_GUARDED = 2  /* FP64 throughout, with guard bands */
 };
-/* Guard bands: the block carries m/8 extra bands (at least 4, within NPL/2)
+/* Guard bands: the block carries m/4 extra bands (at least 4, within NPL/2)
  * and convergence is decided on the requested m.  Without them the block
  * iteration converges on the last requested band at the rate set by its gap
  * to the first unrequested one, and when the band count cuts a degenerate
