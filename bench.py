@@ -68,10 +68,11 @@ def parse():
     p.add_argument("--cpu-samples", type=int, default=3)
     p.add_argument("--no-check", action="store_true",
                    help="skip the dense FP64 reference eigenvalues (|d eps| reported as null)")
-    p.add_argument("--kernel", default=None, choices=["gemm", "forces"],
+    p.add_argument("--kernel", default=None, choices=["gemm", "forces", "local"],
                    help="micro-benchmark one kernel on the workload's shapes instead of the solve (gemm: the "
                         "tensor-core complex GEMM on the mixed phase's subspace shapes, synthetic operands; "
-                        "forces: the FP64 force adjoint and one FP64 operator sweep on seeded bands)")
+                        "forces: the FP64 force adjoint and one FP64 operator sweep on seeded bands; "
+                        "local: the FP32 operator sweep of the mixed mode on seeded bands)")
     p.add_argument("--reps", type=int, default=10, help="repetitions per shape of --kernel")
     p.add_argument("--quick", action="store_true",
                    help="only the timed mixed steps (profiling runs): no dense check, FP64 comparisons, e2e, "
@@ -357,6 +358,37 @@ def run_forces_kernel(args):
                       "flops_convention": "4 x 8 N_pw N_p m (c and three dc as complex products)"}), flush=True)
 
 
+def run_local_kernel(args):
+    """--kernel local: the mixed mode's FP32 H/S sweep (half_apply_hs) on the
+    workload's bands, seeded, at its first k point; the local part's device
+    ms and algorithmic bytes from the library's own events and counters."""
+    import halfb200
+    from halfb200 import synth
+    w = synth.workload(args.workload)
+    ch, po = write_inputs(w, 0)
+    peaks, kind = measured_peaks()
+    with halfb200.Context(ch, po, w.encut, xc=w.xc, solver="acc") as ctx:
+        k = w.kpoints[0]
+        n = ctx.npw(k)
+        r = np.random.default_rng(4)
+        psi = (r.normal(size=(n, w.nbands)) + 1j * r.normal(size=(n, w.nbands))) / np.sqrt(2.0 * n)
+        ctx.set_acc(precision="mixed")
+        loc_ms, loc_b, sweep = [], [], []
+        for i in range(args.warmup + args.reps):
+            ctx.apply_hs(k, psi)
+            inf = ctx.info()
+            if i >= args.warmup:
+                loc_ms.append(inf["local_ms"])
+                loc_b.append(inf["local_bytes"])
+                sweep.append(inf["sweep_ms"])
+    lm, lb = statistics.mean(loc_ms), statistics.mean(loc_b)
+    gbs = lb / (lm * 1e-3) / 1e9
+    print(json.dumps({"kernel": "k1_sphere_to_planes / k2_xlines / k3_planes_to_sphere (FP32)", "workload": w.name,
+                      "npw": n, "bands": w.nbands, "local_ms": lm, "sweep_ms": statistics.mean(sweep),
+                      "algorithmic_gbs": gbs, "peak_gbs": peaks.get("hbm_gbs"),
+                      "frac": gbs / peaks["hbm_gbs"], "peak_source": kind}), flush=True)
+
+
 def ctx_np(w):
     """Projector columns of a workload: (2 l + 1) per channel per atom."""
     return int(sum(cnt * sum(2 * l + 1 for l in sp.lps) for sp, cnt in zip(w.species, w.counts)))
@@ -373,6 +405,9 @@ def main():
         return
     if args.kernel == "forces":
         run_forces_kernel(args)
+        return
+    if args.kernel == "local":
+        run_local_kernel(args)
         return
     import halfb200
     from halfb200 import synth
