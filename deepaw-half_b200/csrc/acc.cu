@@ -735,6 +735,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
   // On the 216-atom cell 235-470 of the 480 requested bands sit at or below
   // the lock tolerance in most iterations of both phases.  Locks are
   // released when the FP32 phase hands over to FP64.
+  // lock tolerance = lock_frac x the phase's tolerance (HALF_LOCK_FRACTION
+  // overrides 0.5: measurement runs)
+  double lock_frac = 0.5;
+  if (const char* lf = std::getenv("HALF_LOCK_FRACTION")) lock_frac = std::min(1.0, std::max(0.0, std::atof(lf)));
   bool hard_lock = soft_lock;
   if (const char* hl = std::getenv("HALF_HARD_LOCK")) hard_lock = soft_lock && std::string(hl) != "0";
   std::vector<int> active;
@@ -801,10 +805,10 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     int since_best = 0;
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run32.residuals(norms, infos);
-      tracer.step("fp32", iter, max_res, norms, mreq, 0.5 * switch_tol);
+      tracer.step("fp32", iter, max_res, norms, mreq, lock_frac * switch_tol);
       if (max_res < 0.9 * best) { best = max_res; since_best = 0; } else { ++since_best; }
       if (max_res <= switch_tol || since_best >= 6) break;
-      advance(run32, 0.5 * switch_tol);
+      advance(run32, lock_frac * switch_tol);
     }
     if (iter > cfg.max_iter) iter = cfg.max_iter;
     op_ms += run32.op_ms;
@@ -817,9 +821,9 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (fp64_iter = 1; fp64_iter <= cfg.max_iter; ++fp64_iter) {
       max_res = run64.residuals(norms, infos);
-      tracer.step("fp64", fp64_iter, max_res, norms, mreq, 0.5 * cfg.tol);
+      tracer.step("fp64", fp64_iter, max_res, norms, mreq, lock_frac * cfg.tol);
       if (max_res <= cfg.tol) { converged = true; break; }
-      advance(run64, 0.5 * cfg.tol);
+      advance(run64, lock_frac * cfg.tol);
     }
     fp64_iter = std::min(fp64_iter, cfg.max_iter);
     iter += fp64_iter;
@@ -830,9 +834,9 @@ void solve_acc(Context& ctx, KOperatorSet& ks, int nbands, bool want_vectors, So
     run64.rayleigh_ritz_x();
     for (iter = 1; iter <= cfg.max_iter; ++iter) {
       max_res = run64.residuals(norms, infos);
-      tracer.step("fp64", iter, max_res, norms, mreq, 0.5 * cfg.tol);
+      tracer.step("fp64", iter, max_res, norms, mreq, lock_frac * cfg.tol);
       if (max_res <= cfg.tol) { converged = true; break; }
-      advance(run64, 0.5 * cfg.tol);
+      advance(run64, lock_frac * cfg.tol);
     }
     iter = std::min(iter, cfg.max_iter);
     fp64_iter = iter;
